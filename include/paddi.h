@@ -1,0 +1,164 @@
+/*
+ * paddi.h -- C ABI of the B200 discord-discovery library (libpaddi.so).
+ *
+ * Drop-in for the per-GPU hot path of PADDi (KraevaYA/PADDi): PD3, the
+ * DRAG-style fixed-length range-discord search, and PALMAD, the MERLIN-style
+ * arbitrary-length search.  All entry points are plain C: pointers, sizes and
+ * status codes, no C++ or framework types.
+ *
+ * Units and conventions follow the reference:
+ *   - a discord is {start index, squared z-normalised distance to its
+ *     nearest non-trivial neighbour}  (struct Discord, src/PALMAD_types.hpp:7-11);
+ *   - the range threshold r is linear; kernels compare squared distances
+ *     against r*r (src/main.cu:144 passes r*r);
+ *   - windows i and j are trivial matches when |i - j| < m - 1
+ *     (src/PD3_kernels.cuh:70);
+ *   - a window is a candidate when no admissible neighbour is closer than
+ *     r, a discord when its nearest-neighbour distance exceeds r
+ *     (src/sets_processing.hpp:28-37); the top-1 is the first maximum.
+ * Where the reference calls exit(1) on a CUDA error (src/common.h:6-16) these
+ * functions return a status; paddi_last_error() gives the message.
+ *
+ * Threading: a context belongs to one host thread at a time and owns one
+ * CUDA stream; use one context per thread for concurrency.
+ */
+#ifndef PADDI_H
+#define PADDI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PADDI_ABI_VERSION 1
+
+typedef enum paddi_status {
+    PADDI_OK = 0,
+    PADDI_ERR_INVALID_ARG = 1,  /* bad pointer, size or length range */
+    PADDI_ERR_CUDA = 2,         /* a CUDA call failed (see paddi_last_error) */
+    PADDI_ERR_OUT_OF_MEMORY = 3,
+    PADDI_ERR_ITER_CAP = 4,     /* the r-schedule did not converge within iter_cap attempts */
+    PADDI_ERR_NO_DEVICE = 5,    /* no CUDA device, or not an sm_100 device */
+    PADDI_ERR_INTERNAL_LIMIT = 6, /* an internal capacity was exceeded */
+    PADDI_ERR_UNSUPPORTED = 7   /* option value not supported by this build */
+} paddi_status;
+
+/* One discord.  Reference: struct Discord {int ind; float dist;} (src/PALMAD_types.hpp:7-11). */
+typedef struct paddi_discord {
+    int32_t ind;  /* start index of the window, -1 when none */
+    float dist;   /* squared z-normalised nn distance, -FLT_MAX when none */
+} paddi_discord;
+
+/* Distance kernel for the dense candidate refine. */
+typedef enum paddi_distance_kernel {
+    PADDI_DIST_AUTO = 0,       /* split-BF16 tensor cores where supported, else FP32 */
+    PADDI_DIST_FP32 = 1,       /* FP32 CUDA cores (the plain form) */
+    PADDI_DIST_SPLIT_BF16 = 2  /* three-term BF16 split on tcgen05 tensor cores */
+} paddi_distance_kernel;
+
+/* Where PALMAD's threshold for the next length comes from. */
+typedef enum paddi_r_policy {
+    PADDI_R_MERLIN = 0,   /* the reference schedule, src/main.cu:136-233 */
+    PADDI_R_LEARNED = 1   /* the learned predictor (paddi_model_*), MERLIN as fallback */
+} paddi_r_policy;
+
+typedef struct paddi_opts {
+    uint32_t struct_size;     /* sizeof(paddi_opts) */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t distance_kernel;  /* paddi_distance_kernel */
+    int32_t r_policy;         /* paddi_r_policy */
+    uint32_t segment_len;     /* phase-1 rows per segment (reference SEGMENT_N); 0 = 512 */
+    uint32_t phase1_chunks;   /* 1024-diagonal chunks a segment scans before the refine; 0 = 4 */
+    uint32_t iter_cap;        /* attempts allowed per length; 0 = 200 */
+    float guard;              /* correlation guard band of the FP32/BF16 decisions; 0 = default */
+} paddi_opts;
+
+/* One (length, r) attempt; the columns of the reference's times table
+ * (src/IOdata.hpp:142-145) plus the values that drive the r-schedule. */
+typedef struct paddi_attempt_log {
+    int32_t m;            /* subsequence length */
+    float r;              /* linear threshold */
+    float r2;             /* r*r, the value the kernels compare against */
+    int32_t found;        /* 1 when the attempt produced the requested discords */
+    int64_t n_cand;       /* "# Candidates": windows never pruned (nn >= r2) */
+    int64_t n_disc;       /* "# Discords": windows with nn > r2 */
+    int64_t n_phase1;     /* candidates left after phase 1 */
+    int32_t n_recheck;    /* windows whose distance was recomputed in FP64 */
+    paddi_discord top;    /* best discord of the attempt */
+    float ms_stats;       /* window statistics (once per length, logged on its first attempt) */
+    float ms_phase1;      /* phase 1 */
+    float ms_refine;      /* compaction + dense refine */
+    float ms_select;      /* classification, FP64 recheck, top-k */
+    float ms_total;       /* the whole attempt */
+} paddi_attempt_log;
+
+typedef struct paddi_ctx paddi_ctx;
+
+/* Library / context management. */
+int32_t paddi_abi_version(void);
+const char *paddi_status_string(paddi_status s);
+void paddi_opts_default(paddi_opts *opts);
+paddi_status paddi_ctx_create(paddi_ctx **ctx, const paddi_opts *opts);
+paddi_status paddi_ctx_destroy(paddi_ctx *ctx);
+const char *paddi_last_error(const paddi_ctx *ctx);
+/* Reserve device memory for series of up to n values and lengths up to maxL
+ * (optional: the entry points grow the reservation on demand). */
+paddi_status paddi_ctx_reserve(paddi_ctx *ctx, size_t n, uint32_t maxL);
+
+/*
+ * PD3: fixed-length discords of length m.
+ * Replaces do_PD3 + node_discords_refine + find_top1_discord
+ * (src/PD3.cuh:15-61, src/sets_processing.hpp:11-46) for one series.
+ *   r > 0 : one attempt at threshold r; out receives up to top_k
+ *           non-overlapping discords with nn > r*r, best first.
+ *   r <= 0: the halving schedule: r starts at 2*sqrt(m) and halves until
+ *           top_k non-overlapping discords exist (the reference's first-length
+ *           loop, src/main.cu:136-156, with the top-k condition of :137).
+ * series: host pointer to n float32 values.  top_k in [1, 16].
+ * log (optional) receives one row per attempt, at most log_cap rows.
+ */
+paddi_status paddi_pd3(paddi_ctx *ctx, const float *series, size_t n, uint32_t m,
+                       uint32_t segment_len, uint32_t top_k, float r, paddi_discord *out,
+                       uint32_t *n_out, paddi_attempt_log *log, uint32_t log_cap,
+                       uint32_t *n_log);
+
+/*
+ * PALMAD: top-1 discord of every length minL..maxL with the MERLIN r-schedule
+ * (src/main.cu:136-233).  out has maxL-minL+1 entries, out[k] for length minL+k.
+ * series: host pointer (paddi_palmad) or device pointer (paddi_palmad_device).
+ */
+paddi_status paddi_palmad(paddi_ctx *ctx, const float *series, size_t n, uint32_t minL,
+                          uint32_t maxL, paddi_discord *out, paddi_attempt_log *log,
+                          uint32_t log_cap, uint32_t *n_log);
+paddi_status paddi_palmad_device(paddi_ctx *ctx, const float *d_series, size_t n, uint32_t minL,
+                                 uint32_t maxL, paddi_discord *out, paddi_attempt_log *log,
+                                 uint32_t log_cap, uint32_t *n_log);
+
+/*
+ * Window statistics of length m on the device, FP32 outputs.
+ * Replaces compute_statistics (src/preprocessing.cuh:68-76): d_mean[i] and
+ * d_std[i] (population) for i < N = n - m + 1, computed from FP64 prefix sums.
+ * stream: a cudaStream_t, or NULL for the context's stream.
+ */
+paddi_status paddi_compute_statistics(paddi_ctx *ctx, const float *d_T, float *d_mean,
+                                      float *d_std, size_t n, uint32_t m, void *stream);
+
+/*
+ * One PD3 attempt on device buffers, with the reference's output arrays.
+ * Replaces do_PD3 (src/PD3.cuh:15-39) followed by node_discords_refine
+ * (src/PD3.cuh:42-50): d_is_cand[i] = 1 iff window i is never pruned
+ * (nn >= r2), d_nnDist[i] = its squared nn distance (FP32 estimate, FP64 near
+ * the threshold) for candidates and -FLT_MAX otherwise.  r2 is squared.
+ * d_T holds n values; d_is_cand / d_nnDist hold n - m + 1 entries.
+ * Returns the candidate count in *n_cand.
+ */
+paddi_status paddi_do_pd3(paddi_ctx *ctx, const float *d_T, size_t n, uint32_t m, float r2,
+                          int32_t *d_is_cand, float *d_nnDist, int64_t *n_cand, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PADDI_H */

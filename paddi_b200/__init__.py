@@ -1,0 +1,241 @@
+"""paddi_b200 -- B200-native discord discovery (PD3 / PALMAD hot path of PADDi).
+
+Python mirror of the C ABI in ``include/paddi.h`` (ctypes over the in-tree
+``libpaddi.so``).  The compute always runs in the CUDA library; there is no
+CPU path.  If the shared library is missing or no sm_100 device is present,
+the calls raise.
+
+Reference entry points and their counterparts here:
+
+=====================================================  ============================
+reference (PADDi src/)                                 paddi_b200
+=====================================================  ============================
+``main`` PALMAD loop, main.cu:136-233                   :func:`palmad`
+``do_PD3`` + refine + ``find_top1_discord``             :func:`pd3`
+``do_PD3`` flags / nnDist on device, PD3.cuh:15         :meth:`Context.do_pd3`
+``compute_statistics``, preprocessing.cuh:68            :meth:`Context.compute_statistics`
+``struct Discord``, PALMAD_types.hpp:7                  :class:`Discord`
+=====================================================  ============================
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpaddi.so")
+
+PADDI_OK = 0
+PADDI_ERR_INVALID_ARG = 1
+PADDI_ERR_CUDA = 2
+PADDI_ERR_OUT_OF_MEMORY = 3
+PADDI_ERR_ITER_CAP = 4
+PADDI_ERR_NO_DEVICE = 5
+PADDI_ERR_INTERNAL_LIMIT = 6
+PADDI_ERR_UNSUPPORTED = 7
+
+DIST_AUTO, DIST_FP32, DIST_SPLIT_BF16 = 0, 1, 2
+R_MERLIN, R_LEARNED = 0, 1
+
+FLT_MAX = float(np.finfo(np.float32).max)
+
+
+class PaddiError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"paddi status {status}: {msg}")
+        self.status = status
+
+
+class _Discord(C.Structure):
+    _fields_ = [("ind", C.c_int32), ("dist", C.c_float)]
+
+
+class _Opts(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32),
+                ("distance_kernel", C.c_int32), ("r_policy", C.c_int32),
+                ("segment_len", C.c_uint32), ("phase1_chunks", C.c_uint32),
+                ("iter_cap", C.c_uint32), ("guard", C.c_float)]
+
+
+class _Log(C.Structure):
+    _fields_ = [("m", C.c_int32), ("r", C.c_float), ("r2", C.c_float), ("found", C.c_int32),
+                ("n_cand", C.c_int64), ("n_disc", C.c_int64), ("n_phase1", C.c_int64),
+                ("n_recheck", C.c_int32), ("top", _Discord), ("ms_stats", C.c_float),
+                ("ms_phase1", C.c_float), ("ms_refine", C.c_float), ("ms_select", C.c_float),
+                ("ms_total", C.c_float)]
+
+    def as_dict(self):
+        return {"m": self.m, "r": self.r, "r2": self.r2, "found": self.found,
+                "n_cand": self.n_cand, "n_disc": self.n_disc, "n_phase1": self.n_phase1,
+                "n_recheck": self.n_recheck, "top_ind": self.top.ind, "top_dist": self.top.dist,
+                "ms_stats": self.ms_stats, "ms_phase1": self.ms_phase1,
+                "ms_refine": self.ms_refine, "ms_select": self.ms_select,
+                "ms_total": self.ms_total}
+
+
+@dataclass(frozen=True)
+class Discord:
+    """A discord: start index and squared z-normalised nn distance."""
+    ind: int
+    dist: float
+
+
+# Every exported function of include/paddi.h with its ctypes signature.
+_SIGS = {
+    "paddi_abi_version": ([], C.c_int32),
+    "paddi_status_string": ([C.c_int], C.c_char_p),
+    "paddi_opts_default": ([C.POINTER(_Opts)], None),
+    "paddi_ctx_create": ([C.POINTER(C.c_void_p), C.POINTER(_Opts)], C.c_int),
+    "paddi_ctx_destroy": ([C.c_void_p], C.c_int),
+    "paddi_last_error": ([C.c_void_p], C.c_char_p),
+    "paddi_ctx_reserve": ([C.c_void_p, C.c_size_t, C.c_uint32], C.c_int),
+    "paddi_pd3": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint32, C.c_uint32,
+                   C.c_float, C.POINTER(_Discord), C.POINTER(C.c_uint32), C.POINTER(_Log),
+                   C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
+    "paddi_palmad": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint32,
+                      C.POINTER(_Discord), C.POINTER(_Log), C.c_uint32,
+                      C.POINTER(C.c_uint32)], C.c_int),
+    "paddi_palmad_device": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint32,
+                             C.POINTER(_Discord), C.POINTER(_Log), C.c_uint32,
+                             C.POINTER(C.c_uint32)], C.c_int),
+    "paddi_compute_statistics": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                  C.c_uint32, C.c_void_p], C.c_int),
+    "paddi_do_pd3": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_float, C.c_void_p,
+                      C.c_void_p, C.POINTER(C.c_int64), C.c_void_p], C.c_int),
+}
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """Load the in-tree CUDA library (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: run __graft_entry__.build() "
+                          "(make -C paddi_b200/csrc)")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _LIB = L
+    return _LIB
+
+
+def status_string(s: int) -> str:
+    return lib().paddi_status_string(s).decode()
+
+
+class Context:
+    """A device context (one stream, device buffers reused across calls)."""
+
+    def __init__(self, device: int = 0, distance_kernel: int = DIST_AUTO,
+                 r_policy: int = R_MERLIN, segment_len: int = 512, phase1_chunks: int = 4,
+                 iter_cap: int = 200, guard: float = 0.0):
+        L = lib()
+        o = _Opts()
+        L.paddi_opts_default(C.byref(o))
+        o.device = device
+        o.distance_kernel = distance_kernel
+        o.r_policy = r_policy
+        o.segment_len = segment_len
+        o.phase1_chunks = phase1_chunks
+        o.iter_cap = iter_cap
+        o.guard = guard
+        h = C.c_void_p()
+        s = L.paddi_ctx_create(C.byref(h), C.byref(o))
+        if s != PADDI_OK:
+            raise PaddiError(s, status_string(s))
+        self._h = h
+        self.opts = o
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().paddi_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, s):
+        if s != PADDI_OK:
+            raise PaddiError(s, lib().paddi_last_error(self._h).decode())
+
+    # ------------------------------------------------------------ drivers
+    def palmad(self, series, minL: int, maxL: int, log_cap: int = 100000):
+        """Top-1 discord of every length minL..maxL; returns (discords, log)."""
+        x = np.ascontiguousarray(series, dtype=np.float32)
+        L = maxL - minL + 1
+        out = (_Discord * max(L, 1))()  # the library rejects an empty range itself
+        log = (_Log * log_cap)()
+        nl = C.c_uint32(0)
+        self._check(lib().paddi_palmad(self._h, x.ctypes.data, len(x), minL, maxL, out, log,
+                                       log_cap, C.byref(nl)))
+        return ([Discord(out[i].ind, out[i].dist) for i in range(L)],
+                [log[i].as_dict() for i in range(min(nl.value, log_cap))])
+
+    def palmad_device(self, d_series_ptr: int, n: int, minL: int, maxL: int,
+                      log_cap: int = 100000):
+        """PALMAD on a series already in device memory (pointer to n floats)."""
+        L = maxL - minL + 1
+        out = (_Discord * max(L, 1))()
+        log = (_Log * log_cap)()
+        nl = C.c_uint32(0)
+        self._check(lib().paddi_palmad_device(self._h, C.c_void_p(d_series_ptr), n, minL, maxL,
+                                              out, log, log_cap, C.byref(nl)))
+        return ([Discord(out[i].ind, out[i].dist) for i in range(L)],
+                [log[i].as_dict() for i in range(min(nl.value, log_cap))])
+
+    def pd3(self, series, m: int, top_k: int = 1, r: float = 0.0, segment_len: int = 0,
+            log_cap: int = 1000):
+        """Fixed-length discords; r <= 0 runs the halving schedule from 2*sqrt(m)."""
+        x = np.ascontiguousarray(series, dtype=np.float32)
+        out = (_Discord * max(top_k, 1))()
+        n_out = C.c_uint32(0)
+        log = (_Log * log_cap)()
+        nl = C.c_uint32(0)
+        self._check(lib().paddi_pd3(self._h, x.ctypes.data, len(x), m, segment_len, top_k,
+                                    float(r), out, C.byref(n_out), log, log_cap, C.byref(nl)))
+        return ([Discord(out[i].ind, out[i].dist) for i in range(n_out.value)],
+                [log[i].as_dict() for i in range(min(nl.value, log_cap))])
+
+    def compute_statistics(self, d_T: int, d_mean: int, d_std: int, n: int, m: int,
+                           stream: int = 0):
+        """Device pointers; reference compute_statistics (src/preprocessing.cuh:68)."""
+        self._check(lib().paddi_compute_statistics(self._h, C.c_void_p(d_T), C.c_void_p(d_mean),
+                                                   C.c_void_p(d_std), n, m,
+                                                   C.c_void_p(stream or None)))
+
+    def do_pd3(self, d_T: int, n: int, m: int, r2: float, d_is_cand: int, d_nnDist: int,
+               stream: int = 0) -> int:
+        """Device pointers; reference do_PD3 + refine (src/PD3.cuh:15-50).  Returns #cand."""
+        nc = C.c_int64(0)
+        self._check(lib().paddi_do_pd3(self._h, C.c_void_p(d_T), n, m, float(r2),
+                                       C.c_void_p(d_is_cand), C.c_void_p(d_nnDist),
+                                       C.byref(nc), C.c_void_p(stream or None)))
+        return nc.value
+
+
+def palmad(series, minL: int, maxL: int, **ctx_kw):
+    """One-shot PALMAD: ``[Discord]`` for lengths minL..maxL and the attempt log."""
+    with Context(**ctx_kw) as c:
+        return c.palmad(series, minL, maxL)
+
+
+def pd3(series, m: int, top_k: int = 1, r: float = 0.0, **ctx_kw):
+    """One-shot PD3 with top-k."""
+    with Context(**ctx_kw) as c:
+        return c.pd3(series, m, top_k=top_k, r=r)

@@ -1,0 +1,133 @@
+// paddi_internal.cuh -- shared device helpers and launch wrappers of the
+// discord-discovery kernels (single GPU, sm_100a).
+//
+// Per-window data for one subsequence length m, laid out in HBM as arrays
+// over the N = n - m + 1 windows (plus PADDI_PAD_WIN zeroed entries so tiles
+// may read past the end without bounds checks):
+//   wst[i]  float4 {df_i, dg_i, inv_i, flat_i}   -- diagonal-update terms
+//           df_i = (x[i+m] - x[i]) / 2,  dg_i = (x[i+m] - mu_{i+1}) + (x[i] - mu_i)
+//           inv_i = 1 / |x_i - mu_i| (0 for a flat window), flat_i in {0, 1}
+//   mu[i]   float  window mean
+//   mu64[i], inv64[i]  FP64 mean and inverse norm (recheck path)
+//   flat[i] uint8
+// The correlation of windows i, j is rho = cov(i,j) * inv_i * inv_j with
+// cov the centred dot product; the squared z-normalised distance is
+// d = 2m (1 - rho) (reference: src/PD3_kernels.cuh:61).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define PADDI_PAD_WIN 4096 /* zeroed tail entries after the last window */
+
+namespace paddi {
+
+// Monotone map float -> uint32 so that unsigned max == float max.
+__device__ __forceinline__ uint32_t f2ord(float f)
+{
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+// Monotone map double -> uint64 (for FP64 atomic min/max).
+__device__ __forceinline__ unsigned long long d2ord(double d)
+{
+    unsigned long long u = (unsigned long long)__double_as_longlong(d);
+    return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ord2d(unsigned long long u)
+{
+    return __longlong_as_double((long long)((u & 0x8000000000000000ull)
+                                                ? (u & 0x7fffffffffffffffull)
+                                                : ~u));
+}
+
+} // namespace paddi
+
+// Per-attempt device-side state shared by the kernels of one (m, r) attempt.
+struct PaddiAttemptDev {
+    int32_t n_cand_p1;      // candidates after phase 1 (compacted list length)
+    int32_t work_next;      // work-item counter of the refine kernel
+    int32_t recheck_next;   // work-item counter of the FP64 recheck kernel
+    int32_t n_recheck;      // windows queued for the FP64 recheck
+    int32_t status;         // nonzero: a kernel hit an internal limit
+    int32_t task_next;      // task counter of the phase-1 kernel
+    unsigned long long n_pairs; // pairs evaluated by the refine (instrumentation)
+};
+
+// Result of one attempt, copied to the host at the end of the attempt.
+struct PaddiAttemptResult {
+    int64_t n_cand;  // windows with nn >= r2 (never pruned)
+    int64_t n_disc;  // windows with nn > r2
+    int32_t n_sel;   // discords selected (<= top_k)
+    int32_t n_recheck;
+    int32_t n_p1;    // candidates after phase 1
+    int32_t status;
+    int32_t sel_ind[16];
+    float sel_dist[16];
+};
+
+#define PADDI_MAX_TOPK 16
+#define PADDI_MAX_RECHECK 1024
+
+// ---------------------------------------------------------------- launches
+// All launch wrappers enqueue on `st` and return cudaGetLastError().
+cudaError_t paddi_launch_stats(const float *x, int64_t n, int32_t m, float4 *wst, float *mu,
+                               double *mu64, double *inv64, uint8_t *flat,
+                               int32_t *flat_count, cudaStream_t st);
+
+cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const float *mu,
+                                    uint8_t *alive, int32_t N, int32_t m, int32_t R,
+                                    int32_t max_chunks, float thr_prune,
+                                    const int32_t *flat_count, int32_t *task_counter,
+                                    int32_t num_sms, cudaStream_t st);
+
+cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
+                                 uint32_t *rho_max, uint8_t *pruned, int32_t *rc_slot,
+                                 PaddiAttemptDev *att, cudaStream_t st);
+
+cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const float *mu,
+                                     const int32_t *cand, PaddiAttemptDev *att,
+                                     uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
+                                     float thr_prune, int32_t num_sms, cudaStream_t st);
+
+cudaError_t paddi_launch_refine_umma(const float *x, const float4 *wst, const float *mu,
+                                     const int32_t *cand, PaddiAttemptDev *att,
+                                     uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
+                                     float thr_prune, int32_t num_sms, cudaStream_t st);
+
+cudaError_t paddi_launch_finalize(const int32_t *cand, PaddiAttemptDev *att,
+                                  const uint32_t *rho_max, const uint8_t *pruned, int32_t m,
+                                  float r2, float thr, float guard, float widen, int32_t top_k,
+                                  const uint8_t *flat, int32_t *recheck, int32_t *rc_slot,
+                                  unsigned long long *nn64_ord, PaddiAttemptResult *res,
+                                  cudaStream_t st);
+
+cudaError_t paddi_launch_recheck(const float *x, const double *mu64, const double *inv64,
+                                 const uint8_t *flat, int32_t N, int32_t m,
+                                 const int32_t *cand, const int32_t *recheck,
+                                 PaddiAttemptDev *att, unsigned long long *nn64_ord,
+                                 int32_t num_sms, int32_t splits, cudaStream_t st);
+
+cudaError_t paddi_launch_select(const int32_t *cand, PaddiAttemptDev *att,
+                                const uint32_t *rho_max, const uint8_t *pruned,
+                                const int32_t *recheck, const int32_t *rc_slot,
+                                const unsigned long long *nn64_ord, int32_t m, float r2,
+                                float thr, float guard, int32_t top_k, const uint8_t *flat,
+                                PaddiAttemptResult *res, cudaStream_t st);
+
+size_t paddi_phase1_smem(int R, int m);
+
+cudaError_t paddi_launch_export_stats(const double *mu64, const double *inv64, int32_t N,
+                                      int32_t m, float *mean, float *sd, cudaStream_t st);
+
+cudaError_t paddi_launch_scatter(const int32_t *cand, const PaddiAttemptDev *att,
+                                 const uint32_t *rho_max, const uint8_t *pruned,
+                                 const int32_t *rc_slot, const unsigned long long *nn64_ord,
+                                 const uint8_t *flat, int32_t N, int32_t m, float r2,
+                                 int32_t *is_cand, float *nnd, cudaStream_t st);
+
+// True when the tcgen05 split-BF16 refine can run on `device`.
+bool paddi_umma_supported(int device);

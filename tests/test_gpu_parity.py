@@ -1,0 +1,197 @@
+"""GPU parity: libpaddi (through its C ABI) against the FP64 oracle.
+
+Every case runs the CUDA library and the oracle on the same seeded input.
+Bars: start indices, candidate / discord counts and attempt outcomes are
+exact; reported squared distances agree within 1e-5 relative (they are FP64
+values rounded to float on both sides, so in practice they are identical).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from paddi_b200 import datagen
+
+P = pytest.importorskip("paddi_b200")
+
+pytestmark = pytest.mark.gpu
+
+DIST_RTOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = P.Context(distance_kernel=P.DIST_AUTO)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def ctx32():
+    c = P.Context(distance_kernel=P.DIST_FP32)
+    yield c
+    c.close()
+
+
+def _series(n, seed, kind="pd3"):
+    if kind == "pd3":
+        x, _ = datagen.pd3_series(n=n, seed=seed, n_anom=4, anom_len=min(150, n // 40))
+    else:
+        x, _ = datagen.palmad_series(n=n, seed=seed, n_anom=4, min_len=32, max_len=96)
+    return x
+
+
+def _close(a, b, rtol=DIST_RTOL):
+    return abs(a - b) <= rtol * max(abs(a), abs(b), 1e-30)
+
+
+# ------------------------------------------------------------------ statistics
+@pytest.mark.parametrize("m", [16, 100, 257])
+def test_statistics_match_oracle(ctx, m):
+    import torch
+    x = _series(6000, 3)
+    mu, sd, _ = O.window_stats(x, m)
+    dT = torch.from_numpy(x).cuda()
+    N = len(x) - m + 1
+    dm = torch.empty(N, dtype=torch.float32, device="cuda")
+    ds = torch.empty(N, dtype=torch.float32, device="cuda")
+    ctx.compute_statistics(dT.data_ptr(), dm.data_ptr(), ds.data_ptr(), len(x), m)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(dm.cpu().numpy(), mu, rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(ds.cpu().numpy(), sd, rtol=2e-6, atol=1e-7)
+
+
+# ------------------------------------------------------------- single attempts
+@pytest.mark.parametrize("n,m", [(4096, 32), (8192, 64), (8192, 128)])
+@pytest.mark.parametrize("q", [0.5, 0.99, 0.9995, 1.01])
+def test_pd3_attempt_counts_and_topk(ctx32, n, m, q):
+    x = _series(n, 11 + m)
+    nn, _ = O.nn_profile(x, m)
+    r2 = float(np.float32(np.quantile(nn, q) if q < 1 else nn.max() * q))
+    r = float(np.sqrt(np.float32(r2)))
+    r2f = np.float32(r) * np.float32(r)
+    att, sel = O.select(nn, m, float(r2f), top_k=3)
+    got, log = ctx32.pd3(x, m, top_k=3, r=r)
+    assert len(log) == 1
+    assert log[0]["n_cand"] == att["n_cand"]
+    assert log[0]["n_disc"] == att["n_disc"]
+    assert [d.ind for d in got] == [s[0] for s in sel]
+    for d, s in zip(got, sel):
+        assert _close(d.dist, s[1])
+
+
+def test_pd3_halving_topk4_matches_oracle(ctx):
+    # the fixed-length workload (n=131072, m=128, k=4) at 1/8 scale
+    x, _ = datagen.pd3_series(n=16384, seed=0, n_anom=4, anom_len=150)
+    m = 128
+    want, watt = O.pd3(x, m, top_k=4)
+    got, log = ctx.pd3(x, m, top_k=4)
+    assert [d.ind for d in got] == [w[0] for w in want]
+    for d, w in zip(got, want):
+        assert _close(d.dist, w[1])
+    assert len(log) == len(watt)
+    for a, b in zip(log, watt):
+        assert a["r2"] == pytest.approx(b["r2"], rel=0, abs=0)
+        assert (a["n_cand"], a["n_disc"]) == (b["n_cand"], b["n_disc"])
+
+
+# ---------------------------------------------------------------------- PALMAD
+@pytest.mark.parametrize("kind,n,minL,maxL", [("pd3", 8192, 32, 44), ("palmad", 8192, 40, 52)])
+def test_palmad_matches_oracle(ctx, kind, n, minL, maxL):
+    x = _series(n, 5, kind)
+    want, watt = O.palmad(x, minL, maxL)
+    got, log = ctx.palmad(x, minL, maxL)
+    assert [d.ind for d in got] == [w[0] for w in want]
+    for d, w in zip(got, want):
+        assert _close(d.dist, w[1])
+    assert len(log) == len(watt)
+    for a, b in zip(log, watt):
+        assert a["m"] == b["m"]
+        assert a["r2"] == b["r2"]
+        assert a["found"] == b["found"]
+        assert (a["n_cand"], a["n_disc"]) == (b["n_cand"], b["n_disc"])
+
+
+def test_palmad_fp32_and_auto_agree(ctx, ctx32):
+    x = _series(8192, 9, "palmad")
+    a, la = ctx.palmad(x, 48, 56)
+    b, lb = ctx32.palmad(x, 48, 56)
+    assert a == b
+    assert [(e["n_cand"], e["n_disc"]) for e in la] == [(e["n_cand"], e["n_disc"]) for e in lb]
+
+
+# ------------------------------------------------------------------ edge cases
+def test_flat_windows(ctx):
+    rng = np.random.default_rng(7)
+    x = np.cumsum(rng.standard_normal(6000)).astype(np.float32)
+    x[1000:1100] = x[1000]          # flat run longer than 2m-1 for m=40
+    x[3000:3050] = x[3000]          # a shorter flat run
+    x[4500:4560] = np.float32(2.5)  # another flat run with a different level
+    for m in (24, 40):
+        want, watt = O.pd3(x, m, top_k=2)
+        got, log = ctx.pd3(x, m, top_k=2)
+        assert [d.ind for d in got] == [w[0] for w in want]
+        for d, w in zip(got, want):
+            assert _close(d.dist, w[1])
+        assert [(e["n_cand"], e["n_disc"]) for e in log] == \
+            [(e["n_cand"], e["n_disc"]) for e in watt]
+
+
+def test_shortest_series(ctx):
+    rng = np.random.default_rng(1)
+    m = 50
+    x = np.cumsum(rng.standard_normal(2 * m)).astype(np.float32)
+    want, _ = O.pd3(x, m, top_k=1)
+    got, _ = ctx.pd3(x, m, top_k=1)
+    assert [d.ind for d in got] == [w[0] for w in want]
+
+
+def test_threshold_exactly_at_a_distance(ctx32):
+    x = _series(4096, 21)
+    m = 48
+    nn, _ = O.nn_profile(x, m)
+    top = int(np.argmax(nn))
+    # r2 equal to the float of the top distance: top is a candidate (nn >= r2)
+    # but not a discord (nn > r2 fails)
+    r2 = np.float32(nn[top])
+    r = np.sqrt(r2, dtype=np.float32)
+    while np.float32(r) * np.float32(r) != r2:  # find r with r*r == r2 in float
+        r = np.nextafter(r, np.float32(np.inf) if r * r < r2 else np.float32(0))
+        if abs(float(r * r) - float(r2)) > 1e-3 * float(r2):
+            pytest.skip("no float r with r*r == nn")
+    att, sel = O.select(nn, m, float(r2), top_k=1)
+    got, log = ctx32.pd3(x, m, top_k=1, r=float(r))
+    assert (log[0]["n_cand"], log[0]["n_disc"]) == (att["n_cand"], att["n_disc"])
+    assert [d.ind for d in got] == [s[0] for s in sel]
+
+
+def test_do_pd3_flags(ctx):
+    import torch
+    x = _series(6000, 33)
+    m = 64
+    nn, _ = O.nn_profile(x, m)
+    r2 = float(np.float32(np.quantile(nn, 0.995)))
+    N = len(x) - m + 1
+    dT = torch.from_numpy(x).cuda()
+    cand = torch.full((N,), -7, dtype=torch.int32, device="cuda")
+    nnd = torch.zeros(N, dtype=torch.float32, device="cuda")
+    nc = ctx.do_pd3(dT.data_ptr(), len(x), m, r2, cand.data_ptr(), nnd.data_ptr())
+    torch.cuda.synchronize()
+    want = (nn.astype(np.float32) >= np.float32(r2))
+    got = cand.cpu().numpy().astype(bool)
+    assert nc == int(want.sum())
+    np.testing.assert_array_equal(got, want)
+    d = nnd.cpu().numpy()
+    np.testing.assert_allclose(d[want], nn[want], rtol=1e-3)
+    assert np.all(d[~want] == -np.finfo(np.float32).max)
+
+
+def test_invalid_arguments_return_status(ctx):
+    x = _series(1000, 1)
+    with pytest.raises(P.PaddiError) as e:
+        ctx.pd3(x, 600)          # n < 2m
+    assert e.value.status == P.PADDI_ERR_INVALID_ARG
+    with pytest.raises(P.PaddiError) as e:
+        ctx.palmad(x, 40, 30)    # maxL < minL
+    assert e.value.status == P.PADDI_ERR_INVALID_ARG
+    with pytest.raises(P.PaddiError):
+        ctx.pd3(x, 32, top_k=99)
