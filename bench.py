@@ -1,0 +1,320 @@
+#!/usr/bin/env python3
+"""PALMAD throughput on B200: n = 2^21, lengths 64..512, top-1 per length.
+
+One step = one full PALMAD run (every length 64..512 with the MERLIN
+r-schedule) over the seeded synthetic series of ``datagen.palmad_series``
+(random walk + sinusoid, 16 planted anomalies: noise / flatline / reversal).
+
+Metric: matrix-equivalent pairs per second, i.e. sum over lengths m of
+N_m^2 (N_m = n - m + 1 windows) divided by the time of one PALMAD run.  It
+is the work an all-pairs method would do per run; the seconds per run are
+reported beside it (``ms_per_step``).
+
+Arms:
+  default            libpaddi on the GPU (device-resident series for
+                     ``value``; host buffers through the C ABI for ``e2e``).
+  --impl reference   the reference's own CPU kernels (oracle/_ref, compiled
+                     from PADDi's src/cpu_kernels/cpu_kernels.cpp) on all host
+                     threads, each step a bounded sample of the same series.
+
+Multi-GPU (torchrun): PALMAD on one series does not shard in this build, so
+--gpus N runs N independent replicas (weak scaling); ``value`` sums them.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+N_SERIES = 1 << 21
+MIN_L, MAX_L = 64, 512
+WORKLOAD = "palmad n=2^21 L=64..512 top-1 (16 planted anomalies, seed 1)"
+CPU_SAMPLE_N = 1 << 15          # points per CPU sample slice
+CPU_SAMPLE_LENGTHS = 8          # lengths 64..71
+L2_FLUSH_BYTES = 512 << 20      # > 126 MB L2
+
+
+def matrix_pairs(n: int, minL: int, maxL: int) -> float:
+    return float(sum((n - m + 1) ** 2 for m in range(minL, maxL + 1)))
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs"), d.get("bf16_tflops"), d.get("bf16_tflops_sustained"), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        busy = [v for v in sm if mx and v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------- dist plumbing
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reduce_max(world, v: float) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- CPU reference
+def cpu_reference(x, steps: int, warmup: int, threads: int):
+    from oracle import oracle as O
+    maxl = MIN_L + CPU_SAMPLE_LENGTHS - 1
+    slices = [x[k * CPU_SAMPLE_N:(k + 1) * CPU_SAMPLE_N] for k in range(threads)]
+    pairs = threads * matrix_pairs(CPU_SAMPLE_N, MIN_L, maxl)
+    for _ in range(warmup):
+        O.ref_palmad_many(slices[:1], MIN_L, MIN_L, threads=1)
+    t = time.perf_counter()
+    for _ in range(steps):
+        O.ref_palmad_many(slices, MIN_L, maxl, threads=threads)
+    el = (time.perf_counter() - t) / steps
+    return {"value": pairs / el, "unit": "pairs/s", "cores": threads, "kind": "reference",
+            "sample": f"{threads} slices of {CPU_SAMPLE_N} points of the same series, "
+                      f"lengths {MIN_L}..{maxl}, one slice per thread",
+            "s_per_sample": el}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from paddi_b200 import datagen
+    x, _ = datagen.palmad_series(n=N_SERIES, seed=1)
+    threads = min(os.cpu_count() or 1, N_SERIES // CPU_SAMPLE_N)
+    cb = cpu_reference(x, args.steps, args.warmup, threads)
+    line = {"metric": "PALMAD matrix-equivalent pairs/s (n=2^21, L=64..512, top-1)",
+            "value": cb["value"], "unit": "pairs/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cb["s_per_sample"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD + " (bounded CPU sample)", "n": N_SERIES,
+                       "minL": MIN_L, "maxL": MAX_L},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_paddi(args, world, rank, local):
+    import torch
+
+    import paddi_b200 as P
+    from paddi_b200 import datagen
+
+    torch.cuda.set_device(local)
+    x, _ = datagen.palmad_series(n=args.n, seed=1)
+    n = len(x)
+    dk = {"auto": P.DIST_AUTO, "fp32": P.DIST_FP32, "bf16": P.DIST_SPLIT_BF16}[args.dist]
+    ctx = P.Context(device=local, distance_kernel=dk)
+    ctx.reserve(n, args.maxL)
+    st = torch.cuda.ExternalStream(ctx.stream)
+    d_x = torch.from_numpy(x).to(f"cuda:{local}")
+    h_x = torch.from_numpy(x).pin_memory()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+    pairs = matrix_pairs(n, args.minL, args.maxL)
+
+    def flush_l2(i):
+        with torch.cuda.stream(st):
+            flush.fill_(float(i))
+
+    for i in range(args.warmup):
+        flush_l2(i)
+        ctx.palmad_device(d_x.data_ptr(), n, args.minL, args.maxL)
+    torch.cuda.synchronize()
+
+    # ---- timed: device-resident series, CUDA events on the context's stream
+    logs, ms = [], []
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush_l2(i)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            disc, log = ctx.palmad_device(d_x.data_ptr(), n, args.minL, args.maxL)
+            e1.record(st)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            logs.append(log)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = clk.summary()
+    step_ms = reduce_max(world, float(np.mean(ms)))
+    value = world * pairs / (step_ms / 1e3)
+
+    # ---- end to end: host series through paddi_palmad (H2D inside the call)
+    e2e_ms = []
+    barrier(world)
+    for i in range(max(1, args.steps)):
+        flush_l2(i)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        d2, l2 = ctx.palmad(h_x.numpy(), args.minL, args.maxL)
+        e1.record(st)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_step = reduce_max(world, float(np.mean(e2e_ms)))
+    e2e_value = world * pairs / (e2e_step / 1e3)
+    n_att = len(logs[-1])
+    d2h = n_att * 152  # one attempt result record per attempt
+
+    # ---- roofline of the dominant kernel group (refine or phase 1)
+    last = logs[-1]
+    tot = {k: sum(e[k] for e in last) for k in ("ms_stats", "ms_phase1", "ms_refine",
+                                              "ms_select")}
+    refine_flops = sum(2.0 * e["m"] * e["refine_pairs"] for e in last)
+    hbm, bf16, bf16_s, src = load_peaks()
+    umma = any(e["refine_kernel"] == 2 for e in last)
+    if umma:
+        peak = bf16 / 3.0  # three BF16 products per FP32-accurate product
+        bound, unit, note = "tensor", "TFLOP/s", f"bf16 {src} / 3 (split-BF16 issues 3 MMAs)"
+    else:
+        peak = 148 * 128 * 2 * 1.965e9 / 1e12  # FP32 FMA, nominal
+        bound, unit, note = "fp32-alu", "TFLOP/s", "nominal FP32 FMA peak (no measured figure)"
+    achieved = refine_flops / (tot["ms_refine"] / 1e3) / 1e12 if tot["ms_refine"] > 0 else 0.0
+    roof = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+            "frac": achieved / peak if peak else None, "traffic": None,
+            "kernel": "k_refine_umma" if umma else "k_refine_fp32", "peak_source": note,
+            "phase_ms": tot}
+    launches = sum(e["n_launches"] for lg in logs for e in lg)
+
+    line = {"metric": "PALMAD matrix-equivalent pairs/s (n=2^21, L=64..512, top-1)",
+            "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3->f32" if umma else "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD if (args.n, args.minL, args.maxL) ==
+                       (N_SERIES, MIN_L, MAX_L) else
+                       f"palmad n={args.n} L={args.minL}..{args.maxL}",
+                       "n": args.n, "minL": args.minL, "maxL": args.maxL,
+                       "distance": args.dist, "l2": "flushed between steps (512 MB write)",
+                       "parallelism": f"replicas x{world}", "attempts_per_step": n_att},
+            "roofline": roof, "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": 4 * n,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
+            "gpu_launches": launches}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference(x, 1, 0, min(os.cpu_count() or 1, N_SERIES // CPU_SAMPLE_N))
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["paddi", "reference"], default="paddi")
+    ap.add_argument("--dist", choices=["auto", "fp32", "bf16"], default="auto")
+    ap.add_argument("--n", type=int, default=N_SERIES)
+    ap.add_argument("--minL", type=int, default=MIN_L)
+    ap.add_argument("--maxL", type=int, default=MAX_L)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_paddi(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -92,6 +92,9 @@ typedef struct paddi_attempt_log {
     float ms_refine;      /* compaction + dense refine */
     float ms_select;      /* classification, FP64 recheck, top-k */
     float ms_total;       /* the whole attempt */
+    int64_t refine_pairs; /* (candidate, window) pairs the dense refine evaluated */
+    int32_t n_launches;   /* kernels this attempt launched (statistics included on its first) */
+    int32_t refine_kernel; /* paddi_distance_kernel that ran the refine (1 FP32, 2 split-BF16) */
 } paddi_attempt_log;
 
 typedef struct paddi_ctx paddi_ctx;
@@ -103,6 +106,9 @@ void paddi_opts_default(paddi_opts *opts);
 paddi_status paddi_ctx_create(paddi_ctx **ctx, const paddi_opts *opts);
 paddi_status paddi_ctx_destroy(paddi_ctx *ctx);
 const char *paddi_last_error(const paddi_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t): every kernel of the context
+ * runs on it, so callers can order or time work against it. */
+void *paddi_ctx_stream(paddi_ctx *ctx);
 /* Reserve device memory for series of up to n values and lengths up to maxL
  * (optional: the entry points grow the reservation on demand). */
 paddi_status paddi_ctx_reserve(paddi_ctx *ctx, size_t n, uint32_t maxL);

@@ -65,7 +65,8 @@ class _Log(C.Structure):
                 ("n_cand", C.c_int64), ("n_disc", C.c_int64), ("n_phase1", C.c_int64),
                 ("n_recheck", C.c_int32), ("top", _Discord), ("ms_stats", C.c_float),
                 ("ms_phase1", C.c_float), ("ms_refine", C.c_float), ("ms_select", C.c_float),
-                ("ms_total", C.c_float)]
+                ("ms_total", C.c_float), ("refine_pairs", C.c_int64), ("n_launches", C.c_int32),
+                ("refine_kernel", C.c_int32)]
 
     def as_dict(self):
         return {"m": self.m, "r": self.r, "r2": self.r2, "found": self.found,
@@ -73,7 +74,8 @@ class _Log(C.Structure):
                 "n_recheck": self.n_recheck, "top_ind": self.top.ind, "top_dist": self.top.dist,
                 "ms_stats": self.ms_stats, "ms_phase1": self.ms_phase1,
                 "ms_refine": self.ms_refine, "ms_select": self.ms_select,
-                "ms_total": self.ms_total}
+                "ms_total": self.ms_total, "refine_pairs": self.refine_pairs,
+                "n_launches": self.n_launches, "refine_kernel": self.refine_kernel}
 
 
 @dataclass(frozen=True)
@@ -92,6 +94,7 @@ _SIGS = {
     "paddi_ctx_destroy": ([C.c_void_p], C.c_int),
     "paddi_last_error": ([C.c_void_p], C.c_char_p),
     "paddi_ctx_reserve": ([C.c_void_p, C.c_size_t, C.c_uint32], C.c_int),
+    "paddi_ctx_stream": ([C.c_void_p], C.c_void_p),
     "paddi_pd3": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint32, C.c_uint32,
                    C.c_float, C.POINTER(_Discord), C.POINTER(C.c_uint32), C.POINTER(_Log),
                    C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
@@ -169,6 +172,14 @@ class Context:
 
     def __exit__(self, *a):
         self.close()
+
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return lib().paddi_ctx_stream(self._h) or 0
+
+    def reserve(self, n: int, maxL: int):
+        self._check(lib().paddi_ctx_reserve(self._h, n, maxL))
 
     def _check(self, s):
         if s != PADDI_OK:

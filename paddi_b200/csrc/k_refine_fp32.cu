@@ -49,8 +49,9 @@ struct RfSmem {
 __global__ void __launch_bounds__(RF_THREADS)
 k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
               const float *__restrict__ mu, const int32_t *__restrict__ cand,
+              const int32_t *__restrict__ list, const int32_t *__restrict__ list_count,
               PaddiAttemptDev *att, uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-              float thr, int32_t grid_ctas)
+              int32_t jb, int32_t je, float thr, int32_t grid_ctas)
 {
     extern __shared__ __align__(16) unsigned char rf_smem[];
     const int mpad = (m + 7) & ~7;
@@ -61,17 +62,18 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
     S.cmu = S.cinv + RF_TW;
     S.cflt = S.cmu + RF_TW;
     __shared__ int s_item, s_alive;
-    __shared__ int cw[RF_TC];
+    __shared__ int cw[RF_TC], cp[RF_TC];
     __shared__ float cf[RF_TC], zsum[RF_TC];
     __shared__ uint8_t dead[RF_TC];
 
-    const int C = att->n_cand_p1;
-    if (C <= 0) return;
+    const int C = *list_count;
+    if (C <= 0 || je <= jb) return;
+    const int range = je - jb;
     const int tiles = (C + RF_TC - 1) / RF_TC;
     int splits = (2 * grid_ctas + tiles - 1) / tiles;
-    const int max_splits = max(1, N / (4 * RF_TW));
+    const int max_splits = max(1, range / (4 * RF_TW));
     splits = max(1, min(splits, max_splits));
-    const int span = (((N + splits - 1) / splits) + RF_TW - 1) / RF_TW * RF_TW;
+    const int span = (((range + splits - 1) / splits) + RF_TW - 1) / RF_TW * RF_TW;
     const int total = tiles * splits;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -83,10 +85,12 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
         const int tile = item % tiles, split = item / tiles;
         // ---- candidates of this item
         if (threadIdx.x < RF_TC) {
-            const int pos = tile * RF_TC + threadIdx.x;
-            const bool v = pos < C;
+            const int li = tile * RF_TC + threadIdx.x;
+            const bool v = li < C;
+            const int pos = v ? list[li] : 0;
             const int w = v ? cand[pos] : 0;
             cw[threadIdx.x] = w;
+            cp[threadIdx.x] = pos;
             dead[threadIdx.x] = !v || __ldcg(pruned + pos);
             cf[threadIdx.x] = v ? wst[w].w : 0.f;
         }
@@ -110,7 +114,7 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
             for (int k = 0; k < m; ++k) s += S.zT[k * RF_TC + threadIdx.x];
             zsum[threadIdx.x] = s;
         }
-        const int j_lo = split * span, j_hi = min(N, j_lo + span);
+        const int j_lo = jb + split * span, j_hi = min(je, j_lo + span);
         float rmax[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
         for (int j0 = j_lo; j0 < j_hi; j0 += RF_TW) {
             __syncthreads();
@@ -176,7 +180,7 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
                 const int ci = 4 * warp + c;
                 if (__any_sync(0xffffffffu, hit[c]) && lane == 0 && !dead[ci]) {
                     dead[ci] = 1;
-                    pruned[tile * RF_TC + ci] = 1;
+                    pruned[cp[ci]] = 1;
                 }
             }
             __syncthreads();
@@ -184,10 +188,10 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
             if (threadIdx.x == 0) s_alive = 0;
             __syncthreads();
             if (threadIdx.x < RF_TC) {
-                const int pos = tile * RF_TC + threadIdx.x;
-                if (!dead[threadIdx.x] && pos < C && __ldcg(pruned + pos)) dead[threadIdx.x] = 1;
+                if (!dead[threadIdx.x] && __ldcg(pruned + cp[threadIdx.x])) dead[threadIdx.x] = 1;
                 if (!dead[threadIdx.x]) s_alive = 1;
             }
+            if (threadIdx.x == 0) atomicAdd(&att->n_pairs, (unsigned long long)(RF_TC * RF_TW));
             __syncthreads();
             if (!s_alive) break;
         }
@@ -198,8 +202,8 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
             const int ci = 4 * warp + c;
-            const int pos = tile * RF_TC + ci;
-            if (lane == 0 && pos < C && v > -INFINITY) atomicMax(rho_max + pos, f2ord(v));
+            if (lane == 0 && tile * RF_TC + ci < C && v > -INFINITY)
+                atomicMax(rho_max + cp[ci], f2ord(v));
         }
         __syncthreads();
     }
@@ -208,9 +212,11 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
 } // namespace
 
 cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const float *mu,
-                                     const int32_t *cand, PaddiAttemptDev *att,
+                                     const int32_t *cand, const int32_t *list,
+                                     const int32_t *list_count, PaddiAttemptDev *att,
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     float thr_prune, int32_t num_sms, cudaStream_t st)
+                                     int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
+                                     cudaStream_t st)
 {
     if (m > RF_MAXM) return cudaErrorInvalidValue;
     const int mpad = (m + 7) & ~7;
@@ -224,7 +230,7 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int grid = num_sms * per_sm;
-    k_refine_fp32<<<grid, RF_THREADS, smem, st>>>(x, wst, mu, cand, att, rho_max, pruned, N, m,
-                                                  thr_prune, grid);
+    k_refine_fp32<<<grid, RF_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, att, rho_max,
+                                                  pruned, N, m, jb, je, thr_prune, grid);
     return cudaGetLastError();
 }

@@ -10,7 +10,8 @@ bool paddi_umma_supported(int device)
 }
 
 cudaError_t paddi_launch_refine_umma(const float *, const float4 *, const float *,
-                                     const int32_t *, PaddiAttemptDev *, uint32_t *, uint8_t *,
+                                     const int32_t *, const int32_t *, const int32_t *,
+                                     PaddiAttemptDev *, uint32_t *, uint8_t *, int32_t, int32_t,
                                      int32_t, int32_t, float, int32_t, cudaStream_t)
 {
     return cudaErrorNotSupported;

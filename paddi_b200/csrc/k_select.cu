@@ -62,6 +62,48 @@ k_compact(const uint8_t *__restrict__ alive, int32_t N, int32_t *cand, uint32_t 
     }
 }
 
+// Identity list 0..C-1 of the phase-1 candidates (first refine round).
+__global__ void k_list_init(const PaddiAttemptDev *att, int32_t *list, int32_t *count)
+{
+    const int C = att->n_cand_p1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < C; i += gridDim.x * blockDim.x)
+        list[i] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *count = C;
+}
+
+// Keeps the not-yet-pruned entries of a candidate list (order within a
+// block preserved), so the next refine round works on dense tiles.
+__global__ void __launch_bounds__(CP_THREADS)
+k_list_compact(const int32_t *__restrict__ in, const int32_t *__restrict__ in_count,
+               const uint8_t *__restrict__ pruned, int32_t *out, int32_t *out_count)
+{
+    __shared__ int wcnt[CP_THREADS / 32];
+    __shared__ int base;
+    const int C = *in_count;
+    for (int b0 = blockIdx.x * CP_THREADS; b0 < C; b0 += gridDim.x * CP_THREADS) {
+        const int i = b0 + threadIdx.x;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        const int p = i < C ? in[i] : 0;
+        const bool a = i < C && !pruned[p];
+        const unsigned b = __ballot_sync(0xffffffffu, a);
+        if (lane == 0) wcnt[w] = __popc(b);
+        __syncthreads();
+        if (w == 0) {
+            int v = wcnt[lane], inc = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int t = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += t;
+            }
+            wcnt[lane] = inc - v;
+            if (lane == 31) base = inc ? atomicAdd(out_count, inc) : 0;
+        }
+        __syncthreads();
+        if (a) out[base + wcnt[w] + __popc(b & ((1u << lane) - 1u))] = p;
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ block helpers
 template <int NT>
 __device__ float block_min(float v, float *red)
@@ -386,6 +428,7 @@ k_select(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
         res->n_disc += addd;
         res->n_sel = np;
         res->n_recheck = nr;
+        res->n_pairs = att->n_pairs;
         res->status = att->status ? att->status : (s_need ? 2 : 0);
     }
 }
@@ -423,6 +466,23 @@ __global__ void k_scatter(const int32_t *__restrict__ cand, const PaddiAttemptDe
 }
 
 } // namespace
+
+cudaError_t paddi_launch_list_init(const PaddiAttemptDev *att, int32_t *list, int32_t *count,
+                                   cudaStream_t st)
+{
+    k_list_init<<<256, 256, 0, st>>>(att, list, count);
+    return cudaGetLastError();
+}
+
+cudaError_t paddi_launch_list_compact(const int32_t *in, const int32_t *in_count,
+                                      const uint8_t *pruned, int32_t *out, int32_t *out_count,
+                                      cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(out_count, 0, sizeof(int32_t), st);
+    if (e != cudaSuccess) return e;
+    k_list_compact<<<64, CP_THREADS, 0, st>>>(in, in_count, pruned, out, out_count);
+    return cudaGetLastError();
+}
 
 cudaError_t paddi_launch_scatter(const int32_t *cand, const PaddiAttemptDev *att,
                                  const uint32_t *rho_max, const uint8_t *pruned,

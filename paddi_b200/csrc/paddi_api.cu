@@ -44,6 +44,7 @@ struct paddi_ctx {
     double *d_mu64 = nullptr, *d_inv64 = nullptr;
     uint8_t *d_flat = nullptr, *d_alive = nullptr, *d_pruned = nullptr;
     int32_t *d_cand = nullptr, *d_rcslot = nullptr, *d_recheck = nullptr;
+    int32_t *d_list[2] = {nullptr, nullptr};
     uint32_t *d_rho = nullptr;
     unsigned long long *d_nn64 = nullptr;
     PaddiAttemptDev *d_att = nullptr;
@@ -101,6 +102,8 @@ void free_buffers(paddi_ctx *ctx)
     dfree(ctx->d_recheck);
     dfree(ctx->d_rho);
     dfree(ctx->d_nn64);
+    dfree(ctx->d_list[0]);
+    dfree(ctx->d_list[1]);
     ctx->cap_n = 0;
 }
 
@@ -122,6 +125,8 @@ paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
     CK(cudaMalloc(&ctx->d_cand, sizeof(int32_t) * W));
     CK(cudaMalloc(&ctx->d_rcslot, sizeof(int32_t) * W));
     CK(cudaMalloc(&ctx->d_rho, sizeof(uint32_t) * W));
+    CK(cudaMalloc(&ctx->d_list[0], sizeof(int32_t) * W));
+    CK(cudaMalloc(&ctx->d_list[1], sizeof(int32_t) * W));
     CK(cudaMalloc(&ctx->d_recheck, sizeof(int32_t) * PADDI_MAX_RECHECK));
     CK(cudaMalloc(&ctx->d_nn64, sizeof(unsigned long long) * PADDI_MAX_RECHECK));
     CK(cudaMemsetAsync(ctx->d_wst, 0, sizeof(float4) * W, ctx->st));
@@ -133,6 +138,8 @@ paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
 struct AttemptOut {
     PaddiAttemptResult res;
     float ms_phase1 = 0, ms_refine = 0, ms_select = 0, ms_total = 0;
+    int launches = 0;
+    int kernel = PADDI_DIST_FP32;
 };
 
 float guard_of(const paddi_ctx *ctx)
@@ -175,19 +182,47 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     CK(cudaEventRecord(ctx->ev[0], st));
     CK(cudaMemsetAsync(ctx->d_alive, 1, (size_t)N, st));
     CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
+    int launches = 0;
     CK(paddi_launch_phase1_dev(x, ctx->d_wst, ctx->d_mu, ctx->d_alive, N, m, R, chunks, thr_prune,
                                ctx->d_flatcount, &ctx->d_att->task_next, ctx->num_sms, st));
+    ++launches;
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(paddi_launch_compact(ctx->d_alive, N, ctx->d_cand, ctx->d_rho, ctx->d_pruned,
                             ctx->d_rcslot, ctx->d_att, st));
-    if (use_umma(ctx, m))
-        CK(paddi_launch_refine_umma(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_att,
-                                    ctx->d_rho, ctx->d_pruned, N, m, thr_prune, ctx->num_sms,
-                                    st));
-    else
-        CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_att,
-                                    ctx->d_rho, ctx->d_pruned, N, m, thr_prune, ctx->num_sms,
-                                    st));
+    ++launches;
+    // refine rounds over geometrically growing window ranges; survivors are
+    // re-compacted between rounds so every tile is dense with live candidates
+    CK(paddi_launch_list_init(ctx->d_att, ctx->d_list[0], &ctx->d_att->list_count[0], st));
+    ++launches;
+    const bool umma = use_umma(ctx, m);
+    out->kernel = umma ? PADDI_DIST_SPLIT_BF16 : PADDI_DIST_FP32;
+    const int nrounds = N >= (1 << 16) ? 8 : 1;
+    int jb = 0;
+    for (int rd = 0; rd < nrounds; ++rd) {
+        // range sizes N/128, N/128, N/64, ..., N/2 (the last round takes the rest)
+        int je = rd == nrounds - 1 ? N : jb + (int)((int64_t)N >> (nrounds - (rd == 0 ? 1 : rd)));
+        if (je > N) je = N;
+        const int a = rd & 1, b = a ^ 1;
+        CK(cudaMemsetAsync(&ctx->d_att->work_next, 0, sizeof(int32_t), st));
+        if (umma)
+            CK(paddi_launch_refine_umma(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
+                                        &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,
+                                        ctx->d_pruned, N, m, jb, je, thr_prune, ctx->num_sms,
+                                        st));
+        else
+            CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
+                                        &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,
+                                        ctx->d_pruned, N, m, jb, je, thr_prune, ctx->num_sms,
+                                        st));
+        ++launches;
+        if (rd + 1 < nrounds) {
+            CK(paddi_launch_list_compact(ctx->d_list[a], &ctx->d_att->list_count[a],
+                                         ctx->d_pruned, ctx->d_list[b],
+                                         &ctx->d_att->list_count[b], st));
+            ++launches;
+        }
+        jb = je;
+    }
     CK(cudaEventRecord(ctx->ev[2], st));
     float widen = 2.f;
     for (int pass = 0; pass < 3; ++pass) {
@@ -200,6 +235,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         CK(paddi_launch_select(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned,
                                ctx->d_recheck, ctx->d_rcslot, ctx->d_nn64, m, r2, thr, guard,
                                top_k, ctx->d_flat, ctx->d_res, st));
+        launches += 3;
         CK(cudaEventRecord(ctx->ev[3], st));
         CK(cudaMemcpyAsync(ctx->h_res, ctx->d_res, sizeof(PaddiAttemptResult),
                            cudaMemcpyDeviceToHost, st));
@@ -216,6 +252,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     if (ctx->h_res->status != 0)
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT, "top-k selection did not settle");
     out->res = *ctx->h_res;
+    out->launches = launches;
     CK(cudaEventElapsedTime(&out->ms_phase1, ctx->ev[0], ctx->ev[1]));
     CK(cudaEventElapsedTime(&out->ms_refine, ctx->ev[1], ctx->ev[2]));
     CK(cudaEventElapsedTime(&out->ms_select, ctx->ev[2], ctx->ev[3]));
@@ -247,6 +284,9 @@ void fill_log(paddi_attempt_log *L, int m, float r, float r2, int top_k, const A
     L->ms_refine = a.ms_refine;
     L->ms_select = a.ms_select;
     L->ms_total = a.ms_total + ms_stats;
+    L->refine_pairs = (int64_t)a.res.n_pairs;
+    L->n_launches = a.launches + (ms_stats > 0.f ? 1 : 0);
+    L->refine_kernel = a.kernel;
 }
 
 bool valid_lengths(size_t n, uint32_t minL, uint32_t maxL)
@@ -411,6 +451,8 @@ PADDI_API const char *paddi_last_error(const paddi_ctx *ctx)
 {
     return ctx ? ctx->err.c_str() : "null context";
 }
+
+PADDI_API void *paddi_ctx_stream(paddi_ctx *ctx) { return ctx ? (void *)ctx->st : nullptr; }
 
 PADDI_API paddi_status paddi_ctx_reserve(paddi_ctx *ctx, size_t n, uint32_t maxL)
 {

@@ -54,6 +54,8 @@ struct PaddiAttemptDev {
     int32_t n_recheck;      // windows queued for the FP64 recheck
     int32_t status;         // nonzero: a kernel hit an internal limit
     int32_t task_next;      // task counter of the phase-1 kernel
+    int32_t list_count[2];  // lengths of the ping-pong candidate lists of the refine rounds
+    int32_t pad_;
     unsigned long long n_pairs; // pairs evaluated by the refine (instrumentation)
 };
 
@@ -67,6 +69,7 @@ struct PaddiAttemptResult {
     int32_t status;
     int32_t sel_ind[16];
     float sel_dist[16];
+    unsigned long long n_pairs; // refine pairs evaluated
 };
 
 #define PADDI_MAX_TOPK 16
@@ -88,15 +91,28 @@ cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
                                  uint32_t *rho_max, uint8_t *pruned, int32_t *rc_slot,
                                  PaddiAttemptDev *att, cudaStream_t st);
 
+// Dense refine of the candidates in list[0..*list_count) (positions into
+// cand[]) against the windows [jb, je).
 cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const float *mu,
-                                     const int32_t *cand, PaddiAttemptDev *att,
+                                     const int32_t *cand, const int32_t *list,
+                                     const int32_t *list_count, PaddiAttemptDev *att,
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     float thr_prune, int32_t num_sms, cudaStream_t st);
+                                     int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
+                                     cudaStream_t st);
 
 cudaError_t paddi_launch_refine_umma(const float *x, const float4 *wst, const float *mu,
-                                     const int32_t *cand, PaddiAttemptDev *att,
+                                     const int32_t *cand, const int32_t *list,
+                                     const int32_t *list_count, PaddiAttemptDev *att,
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     float thr_prune, int32_t num_sms, cudaStream_t st);
+                                     int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
+                                     cudaStream_t st);
+
+cudaError_t paddi_launch_list_init(const PaddiAttemptDev *att, int32_t *list, int32_t *count,
+                                   cudaStream_t st);
+
+cudaError_t paddi_launch_list_compact(const int32_t *in, const int32_t *in_count,
+                                      const uint8_t *pruned, int32_t *out, int32_t *out_count,
+                                      cudaStream_t st);
 
 cudaError_t paddi_launch_finalize(const int32_t *cand, PaddiAttemptDev *att,
                                   const uint32_t *rho_max, const uint8_t *pruned, int32_t m,
