@@ -163,6 +163,30 @@ paddi_status paddi_compute_statistics(paddi_ctx *ctx, const float *d_T, float *d
 paddi_status paddi_do_pd3(paddi_ctx *ctx, const float *d_T, size_t n, uint32_t m, float r2,
                           int32_t *d_is_cand, float *d_nnDist, int64_t *n_cand, void *stream);
 
+/* Largest window count (n - m + 1) that paddi_compute_statistics_noalloc accepts. */
+#define PADDI_NOALLOC_MAX_WINDOWS 131072
+
+/*
+ * Window statistics that allocate no device memory.
+ * No counterpart in the reference: it exists for callers that may not let a
+ * library call cudaMalloc, i.e. hosts that own all device memory through their
+ * own allocator (managed-runtime / FFI embeddings, fixed per-tenant budgets)
+ * and latency-critical loops where an allocation could synchronise the device.
+ * Same results as paddi_compute_statistics (d_mean[i], d_std[i] for
+ * i < n - m + 1), computed on the calling thread's current device and on
+ * `stream` (a cudaStream_t; NULL is the default stream).  The kernels' scratch
+ * lives in a fixed array of about 5 MB inside the library, held on every
+ * device that loads the library until the process exits.
+ *   - Limit: n - m + 1 <= PADDI_NOALLOC_MAX_WINDOWS, 3 <= m <= 1024, n >= 2m;
+ *     anything else returns PADDI_ERR_INVALID_ARG and enqueues nothing.
+ *   - The first call on a device looks up the scratch address; make it
+ *     before any stream capture begins on that device.
+ *   - All calls on a device share the scratch: calls whose GPU work overlaps
+ *     (different streams or host threads) race; run them one after another.
+ */
+paddi_status paddi_compute_statistics_noalloc(const float *d_T, float *d_mean, float *d_std,
+                                              size_t n, uint32_t m, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

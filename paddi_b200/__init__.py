@@ -108,7 +108,12 @@ _SIGS = {
                                   C.c_uint32, C.c_void_p], C.c_int),
     "paddi_do_pd3": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_float, C.c_void_p,
                       C.c_void_p, C.POINTER(C.c_int64), C.c_void_p], C.c_int),
+    "paddi_compute_statistics_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                          C.c_uint32, C.c_void_p], C.c_int),
 }
+
+# Largest n - m + 1 accepted by compute_statistics_noalloc (include/paddi.h).
+NOALLOC_MAX_WINDOWS = 131072
 
 _LIB = None
 
@@ -238,6 +243,28 @@ class Context:
                                        C.c_void_p(d_is_cand), C.c_void_p(d_nnDist),
                                        C.byref(nc), C.c_void_p(stream or None)))
         return nc.value
+
+
+def compute_statistics_noalloc(d_T: int, d_mean: int, d_std: int, n: int, m: int,
+                               stream: int = 0) -> None:
+    """Window mean / std of length m without any device allocation.
+
+    For callers that may not let the library allocate device memory (hosts
+    that own every device byte through their own allocator, or loops that
+    cannot afford an allocation's device synchronisation).  Device pointers;
+    runs on the current device.  n - m + 1 must not exceed
+    NOALLOC_MAX_WINDOWS.  The library keeps one fixed scratch array per
+    device: calls whose GPU work overlaps race with each other, and the first
+    call on a device (which looks the array up) should come before any stream
+    capture.
+    """
+    s = lib().paddi_compute_statistics_noalloc(C.c_void_p(d_T), C.c_void_p(d_mean),
+                                               C.c_void_p(d_std), n, m,
+                                               C.c_void_p(stream or None))
+    if s != PADDI_OK:
+        limit = (f" (n - m + 1 = {n - m + 1}, limit {NOALLOC_MAX_WINDOWS})"
+                 if s == PADDI_ERR_INVALID_ARG else "")
+        raise PaddiError(s, status_string(s) + limit)
 
 
 def palmad(series, minL: int, maxL: int, **ctx_kw):
