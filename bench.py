@@ -192,7 +192,8 @@ def run_paddi(args, world, rank, local):
     torch.cuda.set_device(local)
     x, _ = datagen.palmad_series(n=args.n, seed=1)
     n = len(x)
-    dk = {"auto": P.DIST_AUTO, "fp32": P.DIST_FP32, "bf16": P.DIST_SPLIT_BF16}[args.dist]
+    dk = {"auto": P.DIST_AUTO, "fp32": P.DIST_FP32, "bf16": P.DIST_SPLIT_BF16,
+          "fp16": P.DIST_SPLIT_FP16}[args.dist]
     ctx = P.Context(device=local, distance_kernel=dk)
     ctx.reserve(n, args.maxL)
     st = torch.cuda.ExternalStream(ctx.stream)
@@ -298,7 +299,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["paddi", "reference"], default="paddi")
-    ap.add_argument("--dist", choices=["auto", "fp32", "bf16"], default="auto")
+    ap.add_argument("--dist", choices=["auto", "fp32", "bf16", "fp16"], default="auto")
     ap.add_argument("--n", type=int, default=N_SERIES)
     ap.add_argument("--minL", type=int, default=MIN_L)
     ap.add_argument("--maxL", type=int, default=MAX_L)

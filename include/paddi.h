@@ -53,9 +53,10 @@ typedef struct paddi_discord {
 
 /* Distance kernel for the dense candidate refine. */
 typedef enum paddi_distance_kernel {
-    PADDI_DIST_AUTO = 0,       /* split-BF16 tensor cores where supported, else FP32 */
+    PADDI_DIST_AUTO = 0,       /* split-FP16 tensor cores where the length allows, else FP32 */
     PADDI_DIST_FP32 = 1,       /* FP32 CUDA cores (the plain form) */
-    PADDI_DIST_SPLIT_BF16 = 2  /* three-term BF16 split on tcgen05 tensor cores */
+    PADDI_DIST_SPLIT_BF16 = 2, /* three-term BF16 split on tcgen05 tensor cores */
+    PADDI_DIST_SPLIT_FP16 = 3  /* three-term FP16 split (scaled) on tcgen05 tensor cores */
 } paddi_distance_kernel;
 
 /* Where PALMAD's threshold for the next length comes from. */
@@ -94,7 +95,7 @@ typedef struct paddi_attempt_log {
     float ms_total;       /* the whole attempt */
     int64_t refine_pairs; /* (candidate, window) pairs the dense refine evaluated */
     int32_t n_launches;   /* kernels this attempt launched (statistics included on its first) */
-    int32_t refine_kernel; /* paddi_distance_kernel that ran the refine (1 FP32, 2 split-BF16) */
+    int32_t refine_kernel; /* paddi_distance_kernel that ran the refine (1, 2 or 3) */
 } paddi_attempt_log;
 
 typedef struct paddi_ctx paddi_ctx;

@@ -37,7 +37,7 @@ PADDI_ERR_NO_DEVICE = 5
 PADDI_ERR_INTERNAL_LIMIT = 6
 PADDI_ERR_UNSUPPORTED = 7
 
-DIST_AUTO, DIST_FP32, DIST_SPLIT_BF16 = 0, 1, 2
+DIST_AUTO, DIST_FP32, DIST_SPLIT_BF16, DIST_SPLIT_FP16 = 0, 1, 2, 3
 R_MERLIN, R_LEARNED = 0, 1
 
 FLT_MAX = float(np.finfo(np.float32).max)

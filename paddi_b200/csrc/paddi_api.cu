@@ -142,17 +142,21 @@ struct AttemptOut {
     int kernel = PADDI_DIST_FP32;
 };
 
-float guard_of(const paddi_ctx *ctx)
-{
-    if (ctx->opts.guard > 0.f) return ctx->opts.guard;
-    return 1e-4f;
-}
-
-bool use_umma(const paddi_ctx *ctx, int m)
+// Refine kernel for length m: the tensor-core split where the length fits
+// its shared-memory budget, else FP32 CUDA cores.
+int refine_kernel_for(const paddi_ctx *ctx, int m)
 {
     const int k = ctx->opts.distance_kernel;
-    if (k == PADDI_DIST_FP32) return false;
-    return ctx->umma_ok && m <= 1024;
+    if (k == PADDI_DIST_FP32 || !ctx->umma_ok || m > paddi_umma_max_m()) return PADDI_DIST_FP32;
+    return k == PADDI_DIST_SPLIT_BF16 ? PADDI_DIST_SPLIT_BF16 : PADDI_DIST_SPLIT_FP16;
+}
+
+// Correlation guard band of the pruning decisions.  FP32 and split-FP16
+// keep rho within ~1e-5; split-BF16 within ~2e-4 on random-walk slices.
+float guard_of(const paddi_ctx *ctx, int kernel)
+{
+    if (ctx->opts.guard > 0.f) return ctx->opts.guard;
+    return kernel == PADDI_DIST_SPLIT_BF16 ? 1e-3f : 1e-4f;
 }
 
 // Statistics of length m for the series in `x` (n values).
@@ -169,7 +173,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
                          AttemptOut *out)
 {
     const int32_t N = (int32_t)(n - m + 1);
-    const float guard = guard_of(ctx);
+    const int kernel = refine_kernel_for(ctx, m);
+    const float guard = guard_of(ctx, kernel);
     const float thr = (float)(1.0 - (double)r2 / (2.0 * (double)m));
     const float thr_prune = thr + guard;
     int R = (int)ctx->opts.segment_len;
@@ -194,8 +199,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     // re-compacted between rounds so every tile is dense with live candidates
     CK(paddi_launch_list_init(ctx->d_att, ctx->d_list[0], &ctx->d_att->list_count[0], st));
     ++launches;
-    const bool umma = use_umma(ctx, m);
-    out->kernel = umma ? PADDI_DIST_SPLIT_BF16 : PADDI_DIST_FP32;
+    const bool umma = kernel != PADDI_DIST_FP32;
+    out->kernel = kernel;
     const int nrounds = N >= (1 << 16) ? 8 : 1;
     int jb = 0;
     for (int rd = 0; rd < nrounds; ++rd) {
@@ -205,7 +210,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         const int a = rd & 1, b = a ^ 1;
         CK(cudaMemsetAsync(&ctx->d_att->work_next, 0, sizeof(int32_t), st));
         if (umma)
-            CK(paddi_launch_refine_umma(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
+            CK(paddi_launch_refine_umma(kernel == PADDI_DIST_SPLIT_BF16, x, ctx->d_wst, ctx->d_mu,
+                                        ctx->d_cand, ctx->d_list[a],
                                         &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,
                                         ctx->d_pruned, N, m, jb, je, thr_prune, ctx->num_sms,
                                         st));
@@ -246,6 +252,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         CK(cudaMemsetAsync(&ctx->d_att->recheck_next, 0, sizeof(int32_t), st));
         CK(cudaMemsetAsync(&ctx->d_att->status, 0, sizeof(int32_t), st));
     }
+    if (ctx->h_res->status == 3)
+        return fail(ctx, PADDI_ERR_CUDA, "tensor-core refine: a barrier wait timed out");
     if (ctx->h_res->status == 1)
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT,
                     "more windows than the FP64 recheck capacity fall inside the guard band");
@@ -411,7 +419,9 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
     }
     ctx->num_sms = prop.multiProcessorCount;
     ctx->umma_ok = paddi_umma_supported(ctx->device);
-    if (ctx->opts.distance_kernel == PADDI_DIST_SPLIT_BF16 && !ctx->umma_ok) {
+    if ((ctx->opts.distance_kernel == PADDI_DIST_SPLIT_BF16 ||
+         ctx->opts.distance_kernel == PADDI_DIST_SPLIT_FP16) &&
+        !ctx->umma_ok) {
         delete ctx;
         return PADDI_ERR_UNSUPPORTED;
     }

@@ -100,8 +100,8 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
                                      int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
                                      cudaStream_t st);
 
-cudaError_t paddi_launch_refine_umma(const float *x, const float4 *wst, const float *mu,
-                                     const int32_t *cand, const int32_t *list,
+cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *wst,
+                                     const float *mu, const int32_t *cand, const int32_t *list,
                                      const int32_t *list_count, PaddiAttemptDev *att,
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
                                      int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
@@ -145,5 +145,6 @@ cudaError_t paddi_launch_scatter(const int32_t *cand, const PaddiAttemptDev *att
                                  const uint8_t *flat, int32_t N, int32_t m, float r2,
                                  int32_t *is_cand, float *nnd, cudaStream_t st);
 
-// True when the tcgen05 split-BF16 refine can run on `device`.
+// True when the tcgen05 split refine can run on `device`; longest m it takes.
 bool paddi_umma_supported(int device);
+int paddi_umma_max_m();

@@ -195,3 +195,24 @@ def test_invalid_arguments_return_status(ctx):
     assert e.value.status == P.PADDI_ERR_INVALID_ARG
     with pytest.raises(P.PaddiError):
         ctx.pd3(x, 32, top_k=99)
+
+
+# ------------------------------------------------- every refine kernel, same answers
+@pytest.mark.parametrize("dist", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("n,m", [(8192, 64), (20000, 200), (12000, 361)])
+def test_refine_kernels_match_oracle(dist, n, m):
+    dk = {"fp32": P.DIST_FP32, "fp16": P.DIST_SPLIT_FP16, "bf16": P.DIST_SPLIT_BF16}[dist]
+    x = _series(n, 100 + m)
+    nn, _ = O.nn_profile(x, m)
+    with P.Context(distance_kernel=dk) as c:
+        for q in (0.99, 0.9995):
+            r2 = float(np.float32(np.quantile(nn, q)))
+            r = float(np.sqrt(np.float32(r2)))
+            r2f = np.float32(r) * np.float32(r)
+            att, sel = O.select(nn, m, float(r2f), top_k=2)
+            got, log = c.pd3(x, m, top_k=2, r=r)
+            assert log[0]["refine_kernel"] == dk
+            assert (log[0]["n_cand"], log[0]["n_disc"]) == (att["n_cand"], att["n_disc"])
+            assert [d.ind for d in got] == [s[0] for s in sel]
+            for d, s in zip(got, sel):
+                assert _close(d.dist, s[1])
