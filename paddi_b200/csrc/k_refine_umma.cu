@@ -45,11 +45,11 @@ using paddi::f2ord;
 namespace {
 
 constexpr int UM_THREADS = 256;  // 8 warps
-constexpr int UM_TC = 16;        // candidates per tile
-constexpr int UM_M = 128;        // 16 candidates x 8 shifts
+constexpr int UM_TCMAX = 16;     // candidates per tile (M = 128); 8 for M = 64
 constexpr int UM_N = 256;        // windows at stride 8
 constexpr int UM_TW = UM_N * 8;  // windows per tile
-constexpr int UM_KMAX = 368;     // largest K' (shared-memory bound)
+constexpr int UM_KMAX128 = 368;  // largest K' with M = 128 (shared-memory bound)
+constexpr int UM_KMAX64 = 736;   // largest K' with M = 64
 constexpr int ZSCALE = 8;        // zhat scaled by 2^8 before splitting
 constexpr long long UM_WAIT_CYCLES = 4000000000ll; // ~2 s at 1.9 GHz
 
@@ -166,10 +166,10 @@ struct UmLayout {
     uint32_t a_hi, a_lo, b[2][2], wd, bytes;
 };
 
-__host__ __device__ inline UmLayout um_layout(int kp)
+__host__ __device__ inline UmLayout um_layout(int MM, int kp)
 {
     UmLayout L;
-    const uint32_t a_bytes = (uint32_t)UM_M * kp * 2;
+    const uint32_t a_bytes = (uint32_t)MM * kp * 2;
     const uint32_t b_bytes = ((uint32_t)(UM_TW + kp + 16) * 2 + 127) & ~127u;
     L.a_hi = 0;
     L.a_lo = a_bytes;
@@ -191,10 +191,10 @@ struct UmShared {
     int item, abort, alive;
     float sh[3];     // shift of the tile held by each stage (and the next one)
     float dscale[3]; // 2^-(ZSCALE + e) of the tile
-    int cw[UM_TC], cp[UM_TC];
-    float cflat[UM_TC], zsum[UM_TC];
-    uint32_t rmax[UM_TC];
-    uint8_t dead[UM_TC];
+    int cw[UM_TCMAX], cp[UM_TCMAX];
+    float cflat[UM_TCMAX], zsum[UM_TCMAX];
+    uint32_t rmax[UM_TCMAX];
+    uint8_t dead[UM_TCMAX];
 };
 
 // Converts the slice of the tile starting at window j0 into stage buffers.
@@ -242,7 +242,10 @@ __device__ void um_convert(unsigned char *smem, const UmLayout &L, int stage, co
     }
 }
 
-template <bool BF>
+// MM = 128: 16 candidates, accumulator row r in TMEM lane r.
+// MM = 64:  8 candidates, accumulator row r in TMEM lane (r % 16) + 32 (r / 16)
+//           (lanes 16..31 of every subpartition stay unused).
+template <bool BF, int MM>
 __global__ void __launch_bounds__(UM_THREADS, 1)
 k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
               const float *__restrict__ mu, const int32_t *__restrict__ cand,
@@ -251,11 +254,14 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
               int32_t jb, int32_t je, float thr, int32_t grid_ctas)
 {
     using X = E16<BF>;
+    constexpr int UM_M = MM;
+    constexpr int UM_TC = MM / 8;
+    constexpr int RG = MM / 8;          // 8-row core-matrix groups of A
     extern __shared__ __align__(1024) unsigned char um_smem[];
     __shared__ UmShared S;
     __shared__ float red[UM_THREADS / 32];
     const int kp = kpad_of(m);
-    const UmLayout L = um_layout(kp);
+    const UmLayout L = um_layout(MM, kp);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t nser = (int64_t)N + m - 1;
 
@@ -292,7 +298,9 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
     const int kblocks = kp / 16;
     // epilogue geometry: lane group g (TMEM lanes 32g..32g+31), column half h
     const int g = warp & 3, hcol = warp >> 2;
-    const int row = 32 * g + lane, cidx = row >> 3, bsh = row & 7;
+    const bool rowok = MM == 128 || lane < 16;
+    const int row = MM == 128 ? 32 * g + lane : 16 * g + (lane & 15);
+    const int cidx = row >> 3, bsh = row & 7;
 
     for (;;) {
         if (threadIdx.x == 0) S.item = atomicAdd(&att->work_next, 1);
@@ -326,8 +334,8 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             typename X::T *zh = reinterpret_cast<typename X::T *>(um_smem + L.b[0][0]);
             typename X::T *zl = zh + UM_TC * kp; // aliases the stage buffers (idle here)
             const int c = threadIdx.x >> 4, t16 = threadIdx.x & 15;
-            const int w = S.cw[c];
-            const bool live = !S.dead[c];
+            const int w = c < UM_TC ? S.cw[c] : 0;
+            const bool live = c < UM_TC && !S.dead[c];
             const float muc = live ? mu[w] : 0.f;
             const float ivc = live ? wst[w].z * 256.f : 0.f; // 2^ZSCALE
             float zs = 0.f;
@@ -335,19 +343,21 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 const float v = (live && k < m) ? (x[w + k] - muc) * ivc : 0.f;
                 const typename X::T h = X::cvt(v);
                 const typename X::T l = X::cvt(v - X::back(h));
-                zh[c * kp + k] = h;
-                zl[c * kp + k] = l;
+                if (c < UM_TC) {
+                    zh[c * kp + k] = h;
+                    zl[c * kp + k] = l;
+                }
                 zs += X::back(h) + X::back(l);
             }
 #pragma unroll
             for (int o = 8; o > 0; o >>= 1) zs += __shfl_xor_sync(0xffffffffu, zs, o);
-            if (t16 == 0) S.zsum[c] = zs * (1.f / 256.f);
+            if (t16 == 0 && c < UM_TC) S.zsum[c] = zs * (1.f / 256.f);
             __syncthreads();
             // A[(c,b), k'] = z_c[k' - b] in K-major core matrices:
-            // byte offset ((k'/8)*16 + r/8)*128 + (r%8)*16 + (k'%8)*2
+            // byte offset ((k'/8)*RG + r/8)*128 + (r%8)*16 + (k'%8)*2
             const int chunks = kp / 8;
             for (int e = threadIdx.x; e < UM_M * chunks; e += UM_THREADS) {
-                const int r = e & (UM_M - 1), kc = e >> 7;
+                const int r = e & (UM_M - 1), kc = e / UM_M;
                 const int cc = r >> 3, b = r & 7;
                 uint32_t ph[4], pl[4];
 #pragma unroll
@@ -368,7 +378,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                     pl[q] = (uint32_t)reinterpret_cast<uint16_t &>(l0) |
                             ((uint32_t)reinterpret_cast<uint16_t &>(l1) << 16);
                 }
-                const uint32_t off = (uint32_t)((kc * 16 + (r >> 3)) * 128 + (r & 7) * 16);
+                const uint32_t off = (uint32_t)((kc * RG + (r >> 3)) * 128 + (r & 7) * 16);
                 *reinterpret_cast<uint4 *>(um_smem + L.a_hi + off) =
                     make_uint4(ph[0], ph[1], ph[2], ph[3]);
                 *reinterpret_cast<uint4 *>(um_smem + L.a_lo + off) =
@@ -386,8 +396,9 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             const uint32_t d = tmem + (uint32_t)(s * UM_N);
             const uint32_t bh = smem_u32(um_smem + L.b[s][0]), bl = smem_u32(um_smem + L.b[s][1]);
             for (int kb = 0; kb < kblocks; ++kb) {
-                const uint64_t ah = sdesc(a_hi_s + kb * 4096, 2048, 128);
-                const uint64_t al = sdesc(a_lo_s + kb * 4096, 2048, 128);
+                // K-block kb = core-matrix columns 2kb, 2kb+1; LBO = next K column of cores
+                const uint64_t ah = sdesc(a_hi_s + kb * (2 * RG * 128), RG * 128, 128);
+                const uint64_t al = sdesc(a_lo_s + kb * (2 * RG * 128), RG * 128, 128);
                 const uint64_t bhd = sdesc(bh + kb * 32, 16, 128);
                 const uint64_t bld = sdesc(bl + kb * 32, 16, 128);
                 umma_f16(d, ah, bhd, idesc, kb > 0 ? 1u : 0u);
@@ -459,7 +470,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                     const float ff = (fc != 0.f && wv.y == 0.f) ? 1.f : 0.f;
                     const float rho = fmaf(fmaf(-zsc, wv.x - sh, raw), wv.y, ff);
                     const int dd = wc > j ? wc - j : j - wc;
-                    if (j < j_hi && dd >= m - 1) {
+                    if (rowok && j < j_hi && dd >= m - 1) {
                         rmax = fmaxf(rmax, rho);
                         hit |= rho > thr;
                     }
@@ -467,8 +478,8 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             }
             tc_fence_before();
             const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if (lane < 4 && ((bal >> (8 * lane)) & 0xFFu)) {
-                const int ci = 4 * g + lane;
+            if (lane < UM_TC / 4 && ((bal >> (8 * lane)) & 0xFFu)) {
+                const int ci = (UM_TC / 4) * g + lane;
                 if (!S.dead[ci]) {
                     S.dead[ci] = 1;
                     pruned[S.cp[ci]] = 1;
@@ -513,7 +524,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
         float v = rmax;
 #pragma unroll
         for (int o = 4; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if ((lane & 7) == 0 && v > -INFINITY) atomicMax(&S.rmax[cidx], f2ord(v));
+        if (rowok && (lane & 7) == 0 && v > -INFINITY) atomicMax(&S.rmax[cidx], f2ord(v));
         __syncthreads();
         if (threadIdx.x < UM_TC && tile * UM_TC + threadIdx.x < C &&
             S.rmax[threadIdx.x] != f2ord(-INFINITY))
@@ -542,29 +553,7 @@ bool paddi_umma_supported(int device)
     return p.major == 10 && p.minor == 0; // sm_100 (B200)
 }
 
-int paddi_umma_max_m() { return UM_KMAX - 7; } // kpad_of(m) <= UM_KMAX
-
-cudaError_t paddi_launch_refine_umma_t(bool bf16, const float *x, const float4 *wst,
-                                       const float *mu, const int32_t *cand, const int32_t *list,
-                                       const int32_t *list_count, PaddiAttemptDev *att,
-                                       uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                       int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
-                                       cudaStream_t st)
-{
-    const int kp = kpad_of(m);
-    if (kp > UM_KMAX || m < 3) return cudaErrorInvalidValue;
-    const UmLayout L = um_layout(kp);
-    // request at least half the SM's shared memory so one CTA owns the 512 TMEM columns
-    const size_t smem = L.bytes < 120 * 1024 ? 120 * 1024 : L.bytes;
-    auto kern = bf16 ? k_refine_umma<true> : k_refine_umma<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    const int grid = num_sms;
-    kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, att, rho_max, pruned,
-                                         N, m, jb, je, thr_prune, grid);
-    return cudaGetLastError();
-}
+int paddi_umma_max_m() { return UM_KMAX64 - 7; } // kpad_of(m) <= UM_KMAX64
 
 cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *wst,
                                      const float *mu, const int32_t *cand, const int32_t *list,
@@ -573,6 +562,22 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                                      int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
                                      cudaStream_t st)
 {
-    return paddi_launch_refine_umma_t(bf16, x, wst, mu, cand, list, list_count, att, rho_max,
-                                      pruned, N, m, jb, je, thr_prune, num_sms, st);
+    const int kp = kpad_of(m);
+    if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
+    const int MM = kp <= UM_KMAX128 ? 128 : 64;
+    const UmLayout L = um_layout(MM, kp);
+    // request at least half the SM's shared memory so one CTA owns the 512 TMEM columns
+    const size_t smem = L.bytes < 120 * 1024 ? 120 * 1024 : L.bytes;
+    void (*kern)(const float *, const float4 *, const float *, const int32_t *, const int32_t *,
+                 const int32_t *, PaddiAttemptDev *, uint32_t *, uint8_t *, int32_t, int32_t,
+                 int32_t, int32_t, float, int32_t);
+    if (MM == 128) kern = bf16 ? k_refine_umma<true, 128> : k_refine_umma<false, 128>;
+    else kern = bf16 ? k_refine_umma<true, 64> : k_refine_umma<false, 64>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = num_sms;
+    kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, att, rho_max, pruned,
+                                         N, m, jb, je, thr_prune, grid);
+    return cudaGetLastError();
 }

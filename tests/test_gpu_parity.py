@@ -199,7 +199,8 @@ def test_invalid_arguments_return_status(ctx):
 
 # ------------------------------------------------- every refine kernel, same answers
 @pytest.mark.parametrize("dist", ["fp32", "fp16", "bf16"])
-@pytest.mark.parametrize("n,m", [(8192, 64), (20000, 200), (12000, 361)])
+@pytest.mark.parametrize("n,m", [(8192, 64), (20000, 200), (12000, 361), (12000, 362),
+                                 (16000, 500), (9000, 729)])
 def test_refine_kernels_match_oracle(dist, n, m):
     dk = {"fp32": P.DIST_FP32, "fp16": P.DIST_SPLIT_FP16, "bf16": P.DIST_SPLIT_BF16}[dist]
     x = _series(n, 100 + m)
