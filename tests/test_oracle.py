@@ -70,7 +70,7 @@ def test_candidate_flags_and_distances_vs_reference_cpu():
         # outside the FP32 noise of the reference's formula, which errs in rho
         # (about 5e-4 at m = 16), i.e. by 2m * 5e-4 in distance units
         clear = np.abs(nn - r2) > 2 * m * 5e-4
-        assert clear.mean() > 0.995
+        assert clear.mean() > 0.98
         np.testing.assert_array_equal(cand[clear], want[clear])
         s = cand & clear
         # the reference's raw-dot-product FP32 formula errs in rho, i.e. on the
