@@ -198,6 +198,10 @@ struct UmShared {
 };
 
 // Converts the slice of the tile starting at window j0 into stage buffers.
+// One global read per value: the values stay in registers between the
+// magnitude reduction and the split (at most CV_PER values per thread).
+constexpr int CV_PER = (UM_TW + UM_KMAX64 + 16 + UM_THREADS - 1) / UM_THREADS;
+
 template <bool BF>
 __device__ void um_convert(unsigned char *smem, const UmLayout &L, int stage, const float *x,
                            int64_t nser, int j0, int kp, float *sh_out, float *dscale_out,
@@ -207,12 +211,15 @@ __device__ void um_convert(unsigned char *smem, const UmLayout &L, int stage, co
     typename X::T *hi = reinterpret_cast<typename X::T *>(smem + L.b[stage][0]);
     typename X::T *lo = reinterpret_cast<typename X::T *>(smem + L.b[stage][1]);
     const int cnt = UM_TW + kp + 16;
-    const float sh = x[j0];
+    const float sh = __ldg(x + j0);
+    float v[CV_PER];
     float mx = 0.f;
-    for (int p = threadIdx.x; p < cnt; p += UM_THREADS) {
+#pragma unroll
+    for (int i = 0; i < CV_PER; ++i) {
+        const int p = threadIdx.x + i * UM_THREADS;
         const int64_t g = (int64_t)j0 + p;
-        const float v = g < nser ? x[g] - sh : 0.f;
-        mx = fmaxf(mx, fabsf(v));
+        v[i] = (p < cnt && g < nser) ? __ldg(x + g) - sh : 0.f;
+        mx = fmaxf(mx, fabsf(v[i]));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -229,12 +236,15 @@ __device__ void um_convert(unsigned char *smem, const UmLayout &L, int stage, co
         e = max(-100, min(100, e));
     }
     const float sc = ldexpf(1.f, e);
-    for (int p = threadIdx.x; p < cnt; p += UM_THREADS) {
-        const int64_t g = (int64_t)j0 + p;
-        const float v = g < nser ? (x[g] - sh) * sc : 0.f;
-        const typename X::T h = X::cvt(v);
-        hi[p] = h;
-        lo[p] = X::cvt(v - X::back(h));
+#pragma unroll
+    for (int i = 0; i < CV_PER; ++i) {
+        const int p = threadIdx.x + i * UM_THREADS;
+        if (p < cnt) {
+            const float u = v[i] * sc;
+            const typename X::T h = X::cvt(u);
+            hi[p] = h;
+            lo[p] = X::cvt(u - X::back(h));
+        }
     }
     if (threadIdx.x == 0) {
         *sh_out = sh;
@@ -448,34 +458,54 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                                red);
                 fence_proxy_async_smem();
             }
-            // (mu, inv) of the windows of tile t
+            // per window of tile t: (inv * dscale, (mu - shift) * inv), so that
+            // rho = D * wd.x - zsum_c * wd.y (+1 for two flat windows)
             float2 *wd = reinterpret_cast<float2 *>(um_smem + L.wd);
-            for (int q = threadIdx.x; q < UM_TW; q += UM_THREADS)
-                wd[q] = make_float2(mu[j0 + q], wst[j0 + q].z); // padded tail is zero
+            {
+                float mv[UM_TW / UM_THREADS], iv[UM_TW / UM_THREADS];
+#pragma unroll
+                for (int i = 0; i < UM_TW / UM_THREADS; ++i) {
+                    const int q = threadIdx.x + i * UM_THREADS;
+                    mv[i] = __ldg(mu + j0 + q);    // padded tail is zero
+                    iv[i] = __ldg(&wst[j0 + q].z);
+                }
+#pragma unroll
+                for (int i = 0; i < UM_TW / UM_THREADS; ++i)
+                    wd[threadIdx.x + i * UM_THREADS] = make_float2(iv[i] * dsc, (mv[i] - sh) * iv[i]);
+            }
             __syncthreads();
-            // ---- epilogue: 128 columns per thread
-            bool hit = false;
+            // ---- epilogue: 128 columns per thread; a thread needs the
+            // exclusion / range mask only when its candidate's trivial-match
+            // zone or the end of the item range reaches into the tile
             const uint32_t tb = tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(s * UM_N + 128 * hcol);
+            const bool masked = (j0 + UM_TW > j_hi) || (wc > j0 - m + 1 && wc < j0 + UM_TW + m - 1);
+            float tmax = -INFINITY;
 #pragma unroll 1
             for (int cb = 0; cb < 4; ++cb) {
                 uint32_t r[32];
                 tmem_ld32(tb + 32 * cb, r);
+                const int qb = 8 * (128 * hcol + 32 * cb) + bsh;
+                if (!masked && fc == 0.f) {
 #pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const int a = 128 * hcol + 32 * cb + i;
-                    const int q = 8 * a + bsh;
-                    const int j = j0 + q;
-                    const float2 wv = wd[q];
-                    const float raw = __uint_as_float(r[i]) * dsc;
-                    const float ff = (fc != 0.f && wv.y == 0.f) ? 1.f : 0.f;
-                    const float rho = fmaf(fmaf(-zsc, wv.x - sh, raw), wv.y, ff);
-                    const int dd = wc > j ? wc - j : j - wc;
-                    if (rowok && j < j_hi && dd >= m - 1) {
-                        rmax = fmaxf(rmax, rho);
-                        hit |= rho > thr;
+                    for (int i = 0; i < 32; ++i) {
+                        const float2 wv = wd[qb + 8 * i];
+                        tmax = fmaxf(tmax, fmaf(__uint_as_float(r[i]), wv.x, -zsc * wv.y));
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        const int q = qb + 8 * i, j = j0 + q;
+                        const float2 wv = wd[q];
+                        float rho = fmaf(__uint_as_float(r[i]), wv.x, -zsc * wv.y);
+                        if (fc != 0.f && wv.x == 0.f) rho += 1.f; // two flat windows
+                        const int dd = wc > j ? wc - j : j - wc;
+                        if (j < j_hi && dd >= m - 1) tmax = fmaxf(tmax, rho);
                     }
                 }
             }
+            if (!rowok) tmax = -INFINITY;
+            rmax = fmaxf(rmax, tmax);
+            const bool hit = tmax > thr;
             tc_fence_before();
             const unsigned bal = __ballot_sync(0xffffffffu, hit);
             if (lane < UM_TC / 4 && ((bal >> (8 * lane)) & 0xFFu)) {
@@ -498,16 +528,12 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 }
             }
             // early abandoning: stop once every candidate of the tile is pruned
-            if (threadIdx.x == 0) {
-                int any = 0;
-                for (int c = 0; c < UM_TC; ++c) {
-                    if (!S.dead[c] && __ldcg(pruned + S.cp[c])) S.dead[c] = 1;
-                    any |= !S.dead[c];
-                }
-                S.alive = any;
+            int alive_c = 0;
+            if (threadIdx.x < UM_TC && !S.dead[threadIdx.x]) {
+                if (__ldcg(pruned + S.cp[threadIdx.x])) S.dead[threadIdx.x] = 1;
+                else alive_c = 1;
             }
-            __syncthreads();
-            if (!S.alive) {
+            if (!__syncthreads_or(alive_c)) {
                 if (t + 1 < T) { // drain the MMAs of tile t+1 before leaving the item
                     const int s1 = (t + 1) & 1;
                     if (threadIdx.x == 0 &&
