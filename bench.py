@@ -194,7 +194,8 @@ def run_paddi(args, world, rank, local):
     n = len(x)
     dk = {"auto": P.DIST_AUTO, "fp32": P.DIST_FP32, "bf16": P.DIST_SPLIT_BF16,
           "fp16": P.DIST_SPLIT_FP16}[args.dist]
-    ctx = P.Context(device=local, distance_kernel=dk)
+    rp = {"merlin": P.R_MERLIN, "learned": P.R_LEARNED, "bound": P.R_BOUND}[args.r_policy]
+    ctx = P.Context(device=local, distance_kernel=dk, r_policy=rp)
     ctx.reserve(n, args.maxL)
     st = torch.cuda.ExternalStream(ctx.stream)
     d_x = torch.from_numpy(x).to(f"cuda:{local}")
@@ -298,7 +299,8 @@ def run_paddi(args, world, rank, local):
                        (N_SERIES, MIN_L, MAX_L) else
                        f"palmad n={args.n} L={args.minL}..{args.maxL}",
                        "n": args.n, "minL": args.minL, "maxL": args.maxL,
-                       "distance": args.dist, "l2": "flushed between steps (512 MB write)",
+                       "distance": args.dist, "r_policy": args.r_policy,
+                       "l2": "flushed between steps (512 MB write)",
                        "parallelism": f"replicas x{world}", "attempts_per_step": n_att},
             "roofline": roof, "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": 4 * n,
@@ -319,6 +321,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["paddi", "reference"], default="paddi")
     ap.add_argument("--dist", choices=["auto", "fp32", "bf16", "fp16"], default="auto")
+    ap.add_argument("--r-policy", choices=["merlin", "learned", "bound"], default="merlin")
     ap.add_argument("--n", type=int, default=N_SERIES)
     ap.add_argument("--minL", type=int, default=MIN_L)
     ap.add_argument("--maxL", type=int, default=MAX_L)

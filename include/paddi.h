@@ -62,7 +62,11 @@ typedef enum paddi_distance_kernel {
 /* Where PALMAD's threshold for the next length comes from. */
 typedef enum paddi_r_policy {
     PADDI_R_MERLIN = 0,   /* the reference schedule, src/main.cu:136-233 */
-    PADDI_R_LEARNED = 1   /* the learned predictor (paddi_model_*), MERLIN as fallback */
+    PADDI_R_LEARNED = 1,  /* the learned predictor (paddi_model_*), MERLIN as fallback */
+    PADDI_R_BOUND = 2     /* first try r^2 just below the exact nn, at this length, of the
+                             previous length's top-1 window (a lower bound on this
+                             length's top-1 distance, so the try always succeeds);
+                             MERLIN as fallback */
 } paddi_r_policy;
 
 typedef struct paddi_opts {
@@ -74,7 +78,12 @@ typedef struct paddi_opts {
     uint32_t phase1_chunks;   /* 1024-diagonal chunks a segment scans before the refine; 0 = 4 */
     uint32_t iter_cap;        /* attempts allowed per length; 0 = 200 */
     float guard;              /* correlation guard band of the FP32/BF16 decisions; 0 = default */
+    uint32_t flags;           /* PADDI_FLAG_* */
 } paddi_opts;
+
+/* paddi_opts.flags: compute the bound (paddi_attempt_log.lb) under every r
+ * policy, e.g. to collect training features from plain MERLIN runs. */
+#define PADDI_FLAG_LOG_BOUND 1u
 
 /* One (length, r) attempt; the columns of the reference's times table
  * (src/IOdata.hpp:142-145) plus the values that drive the r-schedule. */
@@ -96,6 +105,11 @@ typedef struct paddi_attempt_log {
     int64_t refine_pairs; /* (candidate, window) pairs the dense refine evaluated */
     int32_t n_launches;   /* kernels this attempt launched (statistics included on its first) */
     int32_t refine_kernel; /* paddi_distance_kernel that ran the refine (1, 2 or 3) */
+    int32_t r_source;     /* where r came from: 0 MERLIN schedule, 1 learned, 2 bound */
+    float ms_guide;       /* time spent choosing r (bound / model), logged on the first attempt */
+    float lb;             /* exact nn at this length of the previous length's top-1 window
+                             (a lower bound on this length's top-1 distance); 0 if not computed */
+    float flat_frac;      /* fraction of flat windows at this length */
 } paddi_attempt_log;
 
 typedef struct paddi_ctx paddi_ctx;
@@ -163,6 +177,37 @@ paddi_status paddi_compute_statistics(paddi_ctx *ctx, const float *d_T, float *d
  */
 paddi_status paddi_do_pd3(paddi_ctx *ctx, const float *d_T, size_t n, uint32_t m, float r2,
                           int32_t *d_is_cand, float *d_nnDist, int64_t *n_cand, void *stream);
+
+/* ------------------------------------------------------------------ learned r
+ * A 12 -> 64 -> 64 -> 1 MLP (GELU) predicts y = log(d_m / d_{m-1}) for the
+ * next length from the previous lengths (no counterpart in the reference, whose
+ * schedule is src/main.cu:136-233).  Its parameters (PADDI_MODEL_NPARAM floats:
+ * W1[64][12] b1[64] W2[64][64] b2[64] W3[64] b3) are trained by the library's
+ * own kernels; inference runs a BF16 copy.  Under PADDI_R_LEARNED the first
+ * attempt of a length uses r^2 = d_{m-1} exp(y_hat) * margin, never below the
+ * bound of PADDI_R_BOUND; a miss is lowered as MERLIN lowers r. */
+#define PADDI_MODEL_NFEAT 12
+#define PADDI_MODEL_NPARAM 5057
+
+/* Features for length minL + j from the top-1 discords of the previous lengths
+ * (out[0..j-1]), the bound lb (0 if unknown), the flat-window fraction and the
+ * number of attempts the previous length took.  Pure host code. */
+paddi_status paddi_r_features(const paddi_discord *out, uint32_t j, uint32_t minL, float lb,
+                              float flat_frac, uint32_t prev_attempts, float *features);
+/* Install model parameters for PADDI_R_LEARNED; margin scales the predicted r^2. */
+paddi_status paddi_model_set(paddi_ctx *ctx, const float *params, uint32_t count, float margin);
+/* Train on n samples (X: n x 12 row-major, Y: n targets) with the pinball loss at
+ * quantile tau, Adam, minibatches, `epochs` passes; params holds the initial
+ * values on entry and the trained ones on return; loss[e] = mean loss of epoch e. */
+paddi_status paddi_model_train(paddi_ctx *ctx, const float *X, const float *Y, uint32_t n,
+                               float tau, uint32_t epochs, uint32_t batch, float lr,
+                               uint64_t seed, float *params, float *loss);
+/* Mean pinball loss and its gradient over the n samples (gradient check). */
+paddi_status paddi_model_grad(paddi_ctx *ctx, const float *X, const float *Y, uint32_t n,
+                              float tau, const float *params, float *grad, float *loss);
+/* Forward pass for n samples with FP32 (bf16 = 0) or BF16 (bf16 = 1) weights. */
+paddi_status paddi_model_predict(paddi_ctx *ctx, const float *X, uint32_t n,
+                                 const float *params, int32_t bf16, float *Y);
 
 /* Largest window count (n - m + 1) that paddi_compute_statistics_noalloc accepts. */
 #define PADDI_NOALLOC_MAX_WINDOWS 131072

@@ -38,7 +38,7 @@ PADDI_ERR_INTERNAL_LIMIT = 6
 PADDI_ERR_UNSUPPORTED = 7
 
 DIST_AUTO, DIST_FP32, DIST_SPLIT_BF16, DIST_SPLIT_FP16 = 0, 1, 2, 3
-R_MERLIN, R_LEARNED = 0, 1
+R_MERLIN, R_LEARNED, R_BOUND = 0, 1, 2
 
 FLT_MAX = float(np.finfo(np.float32).max)
 
@@ -57,7 +57,12 @@ class _Opts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32),
                 ("distance_kernel", C.c_int32), ("r_policy", C.c_int32),
                 ("segment_len", C.c_uint32), ("phase1_chunks", C.c_uint32),
-                ("iter_cap", C.c_uint32), ("guard", C.c_float)]
+                ("iter_cap", C.c_uint32), ("guard", C.c_float), ("flags", C.c_uint32)]
+
+
+FLAG_LOG_BOUND = 1
+MODEL_NFEAT = 12
+MODEL_NPARAM = 5057
 
 
 class _Log(C.Structure):
@@ -66,7 +71,8 @@ class _Log(C.Structure):
                 ("n_recheck", C.c_int32), ("top", _Discord), ("ms_stats", C.c_float),
                 ("ms_phase1", C.c_float), ("ms_refine", C.c_float), ("ms_select", C.c_float),
                 ("ms_total", C.c_float), ("refine_pairs", C.c_int64), ("n_launches", C.c_int32),
-                ("refine_kernel", C.c_int32)]
+                ("refine_kernel", C.c_int32), ("r_source", C.c_int32), ("ms_guide", C.c_float),
+                ("lb", C.c_float), ("flat_frac", C.c_float)]
 
     def as_dict(self):
         return {"m": self.m, "r": self.r, "r2": self.r2, "found": self.found,
@@ -75,7 +81,9 @@ class _Log(C.Structure):
                 "ms_stats": self.ms_stats, "ms_phase1": self.ms_phase1,
                 "ms_refine": self.ms_refine, "ms_select": self.ms_select,
                 "ms_total": self.ms_total, "refine_pairs": self.refine_pairs,
-                "n_launches": self.n_launches, "refine_kernel": self.refine_kernel}
+                "n_launches": self.n_launches, "refine_kernel": self.refine_kernel,
+                "r_source": self.r_source, "ms_guide": self.ms_guide, "lb": self.lb,
+                "flat_frac": self.flat_frac}
 
 
 @dataclass(frozen=True)
@@ -110,6 +118,16 @@ _SIGS = {
                       C.c_void_p, C.POINTER(C.c_int64), C.c_void_p], C.c_int),
     "paddi_compute_statistics_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                           C.c_uint32, C.c_void_p], C.c_int),
+    "paddi_r_features": ([C.POINTER(_Discord), C.c_uint32, C.c_uint32, C.c_float, C.c_float,
+                          C.c_uint32, C.POINTER(C.c_float)], C.c_int),
+    "paddi_model_set": ([C.c_void_p, C.c_void_p, C.c_uint32, C.c_float], C.c_int),
+    "paddi_model_train": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float,
+                           C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, C.c_void_p,
+                           C.c_void_p], C.c_int),
+    "paddi_model_grad": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float,
+                          C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "paddi_model_predict": ([C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int32,
+                             C.c_void_p], C.c_int),
 }
 
 # Largest n - m + 1 accepted by compute_statistics_noalloc (include/paddi.h).
@@ -143,7 +161,9 @@ class Context:
 
     def __init__(self, device: int = 0, distance_kernel: int = DIST_AUTO,
                  r_policy: int = R_MERLIN, segment_len: int = 512, phase1_chunks: int = 4,
-                 iter_cap: int = 200, guard: float = 0.0):
+                 iter_cap: int = 200, guard: float = 0.0, flags: int = 0, model=None,
+                 model_margin: float = 1.0):
+        """model: parameters for R_LEARNED (default: the bundled trained model)."""
         L = lib()
         o = _Opts()
         L.paddi_opts_default(C.byref(o))
@@ -154,12 +174,18 @@ class Context:
         o.phase1_chunks = phase1_chunks
         o.iter_cap = iter_cap
         o.guard = guard
+        o.flags = flags
         h = C.c_void_p()
         s = L.paddi_ctx_create(C.byref(h), C.byref(o))
         if s != PADDI_OK:
             raise PaddiError(s, status_string(s))
         self._h = h
         self.opts = o
+        if r_policy == R_LEARNED:
+            if model is None:
+                from . import learned_r
+                model = learned_r.load_default()
+            self.set_model(model, model_margin)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -185,6 +211,40 @@ class Context:
 
     def reserve(self, n: int, maxL: int):
         self._check(lib().paddi_ctx_reserve(self._h, n, maxL))
+
+    # ------------------------------------------------------------ learned r
+    def set_model(self, params, margin: float = 1.0):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(lib().paddi_model_set(self._h, p.ctypes.data, p.size, float(margin)))
+
+    def model_train(self, X, Y, tau=0.2, epochs=100, batch=4096, lr=3e-3, seed=0, init=None):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        p = np.array(init if init is not None else init_params(seed), dtype=np.float32)
+        loss = np.zeros(max(epochs, 1), np.float32)
+        self._check(lib().paddi_model_train(self._h, X.ctypes.data, Y.ctypes.data, len(Y),
+                                            float(tau), epochs, batch, float(lr), seed,
+                                            p.ctypes.data, loss.ctypes.data))
+        return p, loss[:epochs]
+
+    def model_grad(self, X, Y, params, tau=0.2):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        g = np.zeros(MODEL_NPARAM, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(lib().paddi_model_grad(self._h, X.ctypes.data, Y.ctypes.data, len(Y),
+                                           float(tau), p.ctypes.data, g.ctypes.data,
+                                           loss.ctypes.data))
+        return g, float(loss[0])
+
+    def model_predict(self, X, params, bf16=False):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        y = np.zeros(len(X), np.float32)
+        self._check(lib().paddi_model_predict(self._h, X.ctypes.data, len(X), p.ctypes.data,
+                                              1 if bf16 else 0, y.ctypes.data))
+        return y
 
     def _check(self, s):
         if s != PADDI_OK:
@@ -243,6 +303,33 @@ class Context:
                                        C.c_void_p(d_is_cand), C.c_void_p(d_nnDist),
                                        C.byref(nc), C.c_void_p(stream or None)))
         return nc.value
+
+
+def r_features(discords, j: int, minL: int, lb: float, flat_frac: float,
+               prev_attempts: int) -> np.ndarray:
+    """The learned-r model's 12 features for length minL + j (host code of the
+    library, so training uses exactly what inference uses)."""
+    n = max(j, 1)
+    arr = (_Discord * n)()
+    for i in range(min(j, len(discords))):
+        arr[i].ind = int(discords[i][0] if isinstance(discords[i], tuple) else discords[i].ind)
+        arr[i].dist = float(discords[i][1] if isinstance(discords[i], tuple) else discords[i].dist)
+    f = (C.c_float * MODEL_NFEAT)()
+    s = lib().paddi_r_features(arr, j, minL, float(lb), float(flat_frac), int(prev_attempts), f)
+    if s != PADDI_OK:
+        raise PaddiError(s, status_string(s))
+    return np.array(f[:], dtype=np.float32)
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-style initialisation of the predictor's parameters."""
+    rng = np.random.default_rng(seed)
+    F, H = MODEL_NFEAT, 64
+    w1 = rng.normal(0, np.sqrt(2.0 / F), (H, F))
+    w2 = rng.normal(0, np.sqrt(2.0 / H), (H, H))
+    w3 = rng.normal(0, np.sqrt(1.0 / H), H)
+    return np.concatenate([w1.ravel(), np.zeros(H), w2.ravel(), np.zeros(H), w3,
+                           [0.0]]).astype(np.float32)
 
 
 def compute_statistics_noalloc(d_T: int, d_mean: int, d_std: int, n: int, m: int,

@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(FZ_THREADS)
 k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
            const uint32_t *__restrict__ rho_max, const uint8_t *__restrict__ pruned, int32_t m,
            float r2, float thr, float guard, float widen, int32_t top_k,
-           const uint8_t *__restrict__ flat,
+           const uint8_t *__restrict__ flat, int32_t rc_cap,
            int32_t *recheck, int32_t *rc_slot, unsigned long long *nn64_ord,
            PaddiAttemptResult *res)
 {
@@ -258,7 +258,7 @@ k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
         const bool neartop = np > 0 && r <= cut + widen * guard;
         if (border || neartop) {
             const int k = atomicAdd(&s_nr, 1);
-            if (k < PADDI_MAX_RECHECK) {
+            if (k < rc_cap) {
                 recheck[k] = c;
                 rc_slot[c] = k;
             }
@@ -267,14 +267,15 @@ k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
     __syncthreads();
     if (threadIdx.x == 0) {
         const int nr = s_nr;
-        att->n_recheck = nr < PADDI_MAX_RECHECK ? nr : PADDI_MAX_RECHECK;
-        if (nr > PADDI_MAX_RECHECK) att->status = 1;
+        att->n_recheck = nr < rc_cap ? nr : rc_cap;
+        if (nr > rc_cap) att->status = 1;
         res->n_p1 = C;
+        res->n_recheck = nr;
         res->n_cand = certain_c; // completed in k_select
         res->n_disc = certain_d;
     }
-    for (int k = threadIdx.x; k < PADDI_MAX_RECHECK; k += FZ_THREADS)
-        nn64_ord[k] = d2ord(INFINITY);
+    const int nfill = s_nr < rc_cap ? s_nr : rc_cap;
+    for (int k = threadIdx.x; k < nfill; k += FZ_THREADS) nn64_ord[k] = d2ord(INFINITY);
 }
 
 // ---------------------------------------------------------------- recheck
@@ -508,13 +509,13 @@ cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
 cudaError_t paddi_launch_finalize(const int32_t *cand, PaddiAttemptDev *att,
                                   const uint32_t *rho_max, const uint8_t *pruned, int32_t m,
                                   float r2, float thr, float guard, float widen, int32_t top_k,
-                                  const uint8_t *flat, int32_t *recheck, int32_t *rc_slot,
-                                  unsigned long long *nn64_ord, PaddiAttemptResult *res,
-                                  cudaStream_t st)
+                                  const uint8_t *flat, int32_t rc_cap, int32_t *recheck,
+                                  int32_t *rc_slot, unsigned long long *nn64_ord,
+                                  PaddiAttemptResult *res, cudaStream_t st)
 {
     if (top_k < 1 || top_k > PADDI_MAX_TOPK) return cudaErrorInvalidValue;
     k_finalize<<<1, FZ_THREADS, 0, st>>>(cand, att, rho_max, pruned, m, r2, thr, guard, widen,
-                                         top_k, flat, recheck, rc_slot, nn64_ord, res);
+                                         top_k, flat, rc_cap, recheck, rc_slot, nn64_ord, res);
     return cudaGetLastError();
 }
 

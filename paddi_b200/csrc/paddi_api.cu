@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/paddi.h"
@@ -34,9 +35,10 @@ struct paddi_ctx {
     int device = 0;
     int num_sms = 0;
     cudaStream_t st = nullptr;
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[8] = {};
     std::string err;
     size_t cap_n = 0; // series capacity (values)
+    int32_t rc_cap = 0; // FP64 recheck capacity (windows)
     // device buffers
     float *d_x = nullptr;
     float4 *d_wst = nullptr;
@@ -45,6 +47,20 @@ struct paddi_ctx {
     uint8_t *d_flat = nullptr, *d_alive = nullptr, *d_pruned = nullptr;
     int32_t *d_cand = nullptr, *d_rcslot = nullptr, *d_recheck = nullptr;
     int32_t *d_list[2] = {nullptr, nullptr};
+    // single-window exact nn (r guidance): a one-entry candidate list
+    PaddiAttemptDev *d_att1 = nullptr;
+    int32_t *d_one = nullptr;               // [0] = window, [1] = 0 (recheck slot)
+    unsigned long long *d_nn1 = nullptr;
+    int32_t *h_one = nullptr;               // pinned staging
+    unsigned long long *h_nn1 = nullptr;
+    int32_t *h_flatcount = nullptr;         // pinned
+    // learned r predictor
+    bool model_ok = false;
+    float model_margin = 1.f;
+    float *d_model = nullptr;               // FP32 parameters
+    void *d_model_bf16 = nullptr;           // BF16 copy used for inference
+    float *d_feat = nullptr, *d_pred = nullptr;
+    float *h_feat = nullptr;                // pinned: features [12] then prediction
     uint32_t *d_rho = nullptr;
     unsigned long long *d_nn64 = nullptr;
     PaddiAttemptDev *d_att = nullptr;
@@ -105,6 +121,7 @@ void free_buffers(paddi_ctx *ctx)
     dfree(ctx->d_list[0]);
     dfree(ctx->d_list[1]);
     ctx->cap_n = 0;
+    ctx->rc_cap = 0;
 }
 
 paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
@@ -129,6 +146,7 @@ paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
     CK(cudaMalloc(&ctx->d_list[1], sizeof(int32_t) * W));
     CK(cudaMalloc(&ctx->d_recheck, sizeof(int32_t) * PADDI_MAX_RECHECK));
     CK(cudaMalloc(&ctx->d_nn64, sizeof(unsigned long long) * PADDI_MAX_RECHECK));
+    ctx->rc_cap = PADDI_MAX_RECHECK;
     CK(cudaMemsetAsync(ctx->d_wst, 0, sizeof(float4) * W, ctx->st));
     CK(cudaMemsetAsync(ctx->d_mu, 0, sizeof(float) * W, ctx->st));
     ctx->cap_n = n;
@@ -231,9 +249,9 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     }
     CK(cudaEventRecord(ctx->ev[2], st));
     float widen = 2.f;
-    for (int pass = 0; pass < 3; ++pass) {
+    for (int pass = 0; pass < 6; ++pass) {
         CK(paddi_launch_finalize(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned, m, r2, thr,
-                                 guard, widen, top_k, ctx->d_flat, ctx->d_recheck,
+                                 guard, widen, top_k, ctx->d_flat, ctx->rc_cap, ctx->d_recheck,
                                  ctx->d_rcslot, ctx->d_nn64, ctx->d_res, st));
         CK(paddi_launch_recheck(x, ctx->d_mu64, ctx->d_inv64, ctx->d_flat, N, m, ctx->d_cand,
                                 ctx->d_recheck, ctx->d_att, ctx->d_nn64, ctx->num_sms,
@@ -246,9 +264,21 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         CK(cudaMemcpyAsync(ctx->h_res, ctx->d_res, sizeof(PaddiAttemptResult),
                            cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        if (ctx->h_res->status != 2) break;
-        // a pick had no exact value: queue everything up to the cut and redo
-        widen = 1e30f;
+        if (ctx->h_res->status == 1) {
+            // more windows need the exact value than the queue holds: grow it and redo
+            int32_t cap = ctx->rc_cap;
+            while (cap < ctx->h_res->n_recheck) cap *= 2;
+            dfree(ctx->d_recheck);
+            dfree(ctx->d_nn64);
+            CK(cudaMalloc(&ctx->d_recheck, sizeof(int32_t) * (size_t)cap));
+            CK(cudaMalloc(&ctx->d_nn64, sizeof(unsigned long long) * (size_t)cap));
+            ctx->rc_cap = cap;
+        } else if (ctx->h_res->status == 2) {
+            // a pick had no exact value: queue everything up to the cut and redo
+            widen = 1e30f;
+        } else {
+            break;
+        }
         CK(cudaMemsetAsync(&ctx->d_att->recheck_next, 0, sizeof(int32_t), st));
         CK(cudaMemsetAsync(&ctx->d_att->status, 0, sizeof(int32_t), st));
     }
@@ -256,7 +286,12 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         return fail(ctx, PADDI_ERR_CUDA, "tensor-core refine: a barrier wait timed out");
     if (ctx->h_res->status == 1)
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT,
-                    "more windows than the FP64 recheck capacity fall inside the guard band");
+                    "more windows than the FP64 recheck capacity fall inside the guard band (m=" +
+                        std::to_string(m) + ", r2=" + std::to_string(r2) +
+                        ", phase-1 candidates=" + std::to_string(ctx->h_res->n_p1) +
+                        ", certain=" + std::to_string(ctx->h_res->n_cand) +
+                        ", queued>=" + std::to_string(ctx->h_res->n_recheck) +
+                        ", widen=" + std::to_string(widen) + ")");
     if (ctx->h_res->status != 0)
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT, "top-k selection did not settle");
     out->res = *ctx->h_res;
@@ -295,12 +330,122 @@ void fill_log(paddi_attempt_log *L, int m, float r, float r2, int top_k, const A
     L->refine_pairs = (int64_t)a.res.n_pairs;
     L->n_launches = a.launches + (ms_stats > 0.f ? 1 : 0);
     L->refine_kernel = a.kernel;
+    L->r_source = 0;
+    L->ms_guide = 0.f;
 }
 
 bool valid_lengths(size_t n, uint32_t minL, uint32_t maxL)
 {
     return minL >= 3 && maxL >= minL && maxL <= 1024 && n >= 2 * (size_t)maxL &&
            n < (size_t)INT32_MAX - PADDI_PAD_WIN - 64;
+}
+
+// Exact FP64 nearest-neighbour distance of window w at the length whose
+// statistics are current (the FP64 recheck kernel with a one-entry list).
+paddi_status window_nn64(paddi_ctx *ctx, const float *x, size_t n, int m, int w, double *out)
+{
+    const int32_t N = (int32_t)(n - m + 1);
+    cudaStream_t st = ctx->st;
+    // att1 = {n_cand_p1 = 1, counters 0, n_recheck = 1}
+    PaddiAttemptDev a1;
+    std::memset(&a1, 0, sizeof(a1));
+    a1.n_cand_p1 = 1;
+    a1.n_recheck = 1;
+    static_assert(sizeof(PaddiAttemptDev) <= 4 * sizeof(int32_t) + 64, "staging");
+    ctx->h_one[0] = w;
+    ctx->h_one[1] = 0;
+    CK(cudaMemcpyAsync(ctx->d_one, ctx->h_one, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->d_att1, &a1, sizeof(a1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->d_nn1, 0xff, sizeof(unsigned long long), st)); // +inf image
+    CK(paddi_launch_recheck(x, ctx->d_mu64, ctx->d_inv64, ctx->d_flat, N, m, ctx->d_one,
+                            ctx->d_one + 1, ctx->d_att1, ctx->d_nn1, ctx->num_sms,
+                            ctx->num_sms, st));
+    CK(cudaMemcpyAsync(ctx->h_nn1, ctx->d_nn1, sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const unsigned long long u = *ctx->h_nn1;
+    const unsigned long long bits = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+    double d;
+    std::memcpy(&d, &bits, sizeof(d));
+    *out = d;
+    return PADDI_OK;
+}
+
+// MERLIN's first r for length minL + j (src/main.cu:38, 171, 202-214): a pure
+// function of the previous top-1 distances; S is the decrement of :230.
+float merlin_first_r(const paddi_discord *out, int j, uint32_t minL, float *S_out)
+{
+    float S = 0.f, r;
+    if (j == 0) {
+        r = (float)(2.0 * std::sqrt((double)minL)); // sqrt of an unsigned int: double
+    } else if (j < 5) {
+        r = (float)((double)std::sqrt(out[j - 1].dist) * 0.99); // :171
+    } else {
+        float M = 0.f;
+        for (int k = j - 5; k < j; ++k) M += std::sqrt(out[k].dist); // :205-206
+        M = (float)((double)M * 0.2);                               // :208
+        for (int k = j - 5; k < j; ++k)
+            S = (float)((double)S + std::pow((double)(std::sqrt(out[k].dist) - M), 2.0));
+        S = (float)std::sqrt((double)S * 0.2); // :213
+        r = M - 2 * S;                         // :214
+    }
+    if (S_out) *S_out = S;
+    return r;
+}
+
+// MERLIN's lowering of r after an attempt without discords (:155, :187, :230).
+float merlin_lower(float r, int j, float S)
+{
+    if (j == 0) return (float)(0.5 * (double)r);
+    if (j < 5) return (float)(0.99 * (double)r);
+    return r - S;
+}
+
+// Largest float r with r*r < v (v > 0).
+float r_below(float v)
+{
+    float r = std::sqrt(v);
+    while (r > 0.f && r * r >= v) r = std::nextafter(r, 0.f);
+    return r;
+}
+
+void r_features_impl(const paddi_discord *out, int j, uint32_t minL, float lb, float flat_frac,
+                     int prev_attempts, float *f)
+{
+    const int m = (int)minL + j;
+    auto d = [&](int k) { return (double)std::fmax(out[k].dist, 1e-6f); };
+    auto lr = [&](int a, int b) { return (float)std::log(d(a) / d(b)); };
+    for (int k = 0; k < MLP_NFEAT; ++k) f[k] = 0.f;
+    f[0] = (float)m / 1024.f;
+    if (j >= 1) f[1] = (float)std::log(d(j - 1) / (2.0 * m));
+    if (j >= 2) f[2] = lr(j - 1, j - 2);
+    if (j >= 3) f[3] = lr(j - 2, j - 3);
+    if (j >= 4) f[4] = lr(j - 3, j - 4);
+    if (j >= 1 && lb > 0.f) f[5] = (float)std::log((double)lb / d(j - 1));
+    if (j >= 2) f[6] = out[j - 1].ind != out[j - 2].ind ? 1.f : 0.f;
+    f[7] = (float)std::min(std::max(prev_attempts - 1, 0), 10) / 10.f;
+    if (j >= 1) {
+        float S = 0.f;
+        const float r0 = merlin_first_r(out, j, minL, &S);
+        f[8] = (float)std::log(std::fmax((double)r0 * r0, 1e-6) / d(j - 1));
+        if (j >= 5) f[10] = (float)std::log(std::fmax((double)S, 1e-6) / std::fmax((double)std::fabs(r0) + 2.0 * S, 1e-6));
+    }
+    f[9] = flat_frac;
+    if (j >= 5) f[11] = 0.25f * lr(j - 1, j - 5);
+}
+
+// Prediction of the learned model for one feature vector (BF16 weights).
+paddi_status model_predict1(paddi_ctx *ctx, const float *f, float *y)
+{
+    std::memcpy(ctx->h_feat, f, sizeof(float) * MLP_NFEAT);
+    CK(cudaMemcpyAsync(ctx->d_feat, ctx->h_feat, sizeof(float) * MLP_NFEAT,
+                       cudaMemcpyHostToDevice, ctx->st));
+    CK(paddi_launch_mlp_forward(ctx->d_feat, 1, ctx->d_model_bf16, true, ctx->d_pred, ctx->st));
+    CK(cudaMemcpyAsync(ctx->h_feat + MLP_NFEAT, ctx->d_pred, sizeof(float),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    *y = ctx->h_feat[MLP_NFEAT];
+    return PADDI_OK;
 }
 
 // PALMAD on a series already on the device.
@@ -310,31 +455,71 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
 {
     const int L = (int)(maxL - minL + 1);
     const int iter_cap = ctx->opts.iter_cap ? (int)ctx->opts.iter_cap : 200;
+    const int policy = ctx->opts.r_policy;
+    if (policy == PADDI_R_LEARNED && !ctx->model_ok)
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "r_policy LEARNED needs paddi_model_set first");
+    const bool want_lb = policy != PADDI_R_MERLIN || (ctx->opts.flags & PADDI_FLAG_LOG_BOUND);
     uint32_t nl = 0;
     for (int j = 0; j < L; ++j) {
         out[j].ind = -1;
         out[j].dist = -FLT_MAX;
     }
-    // src/main.cu:38 -- sqrt of an unsigned int is evaluated in double
-    float r = (float)(2.0 * std::sqrt((double)minL));
+    int prev_attempts = 0;
     for (int j = 0; j < L; ++j) {
         const int m = (int)minL + j;
+        const int32_t N = (int32_t)(n - m + 1);
         CK(cudaEventRecord(ctx->ev[4], ctx->st));
         paddi_status s = run_stats(ctx, x, n, m);
         if (s != PADDI_OK) return s;
         CK(cudaEventRecord(ctx->ev[5], ctx->st));
+        CK(cudaMemcpyAsync(ctx->h_flatcount, ctx->d_flatcount, sizeof(int32_t),
+                           cudaMemcpyDeviceToHost, ctx->st));
         float S = 0.f;
-        if (j >= 1 && j < 5) {
-            r = (float)((double)std::sqrt(out[j - 1].dist) * 0.99); // :171
-        } else if (j >= 5) {
-            float M = 0.f;
-            for (int k = j - 5; k < j; ++k) M += std::sqrt(out[k].dist); // :205-206
-            M = (float)((double)M * 0.2);                               // :208
-            for (int k = j - 5; k < j; ++k)
-                S = (float)((double)S + std::pow((double)(std::sqrt(out[k].dist) - M), 2.0));
-            S = (float)std::sqrt((double)S * 0.2); // :213
-            r = M - 2 * S;                         // :214
+        float r = merlin_first_r(out, j, minL, &S);
+        // ---- guidance: the bound and / or the model's prediction
+        float ms_guide = 0.f, lbf = 0.f, lbm = 0.f; // lbm: largest r^2 below the bound
+        int source = 0;
+        if (j >= 1 && out[j - 1].ind >= 0 && (want_lb || policy == PADDI_R_LEARNED)) {
+            // the previous length's top-1 window, evaluated exactly at this length:
+            // its nn is a lower bound on this length's top-1 distance
+            const int w = out[j - 1].ind < N ? out[j - 1].ind : N - 1;
+            CK(cudaEventRecord(ctx->ev[6], ctx->st));
+            double lb = 0.0;
+            s = window_nn64(ctx, x, n, m, w, &lb);
+            if (s != PADDI_OK) return s;
+            if (std::isfinite(lb) && lb > 0.0) {
+                lbf = (float)std::fmin(lb, (double)FLT_MAX);
+                const float rb = r_below(lbf);
+                lbm = rb * rb;
+            }
         }
+        const float flat_frac = (float)*ctx->h_flatcount / (float)N; // synced above when guided
+        if (policy == PADDI_R_BOUND && lbm > 0.f && lbm > r * r) {
+            // tighter than MERLIN's first r and certain to find a discord (a window
+            // that was flat at m-1 may have a small nn at m: then MERLIN leads)
+            r = r_below(lbf);
+            source = 2;
+        } else if (policy == PADDI_R_LEARNED && j >= 1) {
+            float f[MLP_NFEAT];
+            r_features_impl(out, j, minL, lbf, flat_frac, prev_attempts, f);
+            float y = 0.f;
+            s = model_predict1(ctx, f, &y);
+            if (s != PADDI_OK) return s;
+            double r2 = (double)std::fmax(out[j - 1].dist, 1e-6f) * std::exp((double)y) *
+                        (double)ctx->model_margin;
+            if (lbm > 0.f && r2 < (double)lbm) r2 = lbm; // never looser than the bound
+            if (std::isfinite(r2) && r2 > 0.0) {
+                r = r_below((float)std::fmin(r2 * (1.0 + 1e-7), (double)FLT_MAX));
+                if (lbm > 0.f && r * r < lbm) r = r_below(lbf);
+                source = 1;
+            }
+        }
+        if (j >= 1 && (want_lb || policy == PADDI_R_LEARNED)) {
+            CK(cudaEventRecord(ctx->ev[7], ctx->st));
+            CK(cudaEventSynchronize(ctx->ev[7]));
+            CK(cudaEventElapsedTime(&ms_guide, ctx->ev[6], ctx->ev[7]));
+        }
+        // ---- attempts
         int it = 0;
         bool first = true;
         while (out[j].dist < 0) {
@@ -348,17 +533,34 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
             if (s != PADDI_OK) return s;
             float ms_stats = 0.f;
             if (first) CK(cudaEventElapsedTime(&ms_stats, ctx->ev[4], ctx->ev[5]));
-            first = false;
             if (a.res.n_sel > 0) {
                 out[j].ind = a.res.sel_ind[0];
                 out[j].dist = a.res.sel_dist[0];
             }
-            if (log && nl < log_cap) fill_log(&log[nl], m, r, r2, 1, a, ms_stats);
+            if (log && nl < log_cap) {
+                fill_log(&log[nl], m, r, r2, 1, a, ms_stats);
+                log[nl].r_source = source;
+                log[nl].lb = lbf;
+                log[nl].flat_frac = (float)*ctx->h_flatcount / (float)N;
+                if (first) {
+                    log[nl].ms_guide = ms_guide;
+                    log[nl].ms_total += ms_guide;
+                    log[nl].n_launches += (lbf > 0.f ? 1 : 0) + (source == 1 ? 1 : 0);
+                }
+            }
             ++nl;
-            if (j == 0) r = (float)(0.5 * (double)r);       // :155
-            else if (j < 5) r = (float)(0.99 * (double)r);  // :187
-            else r = r - S;                                 // :230
+            first = false;
+            if (out[j].dist >= 0) break;
+            // no discord: lower r as MERLIN does; the guided policies never go below
+            // the bound, where a discord is certain
+            r = merlin_lower(r, j, S);
+            source = 0;
+            if (policy != PADDI_R_MERLIN && lbm > 0.f && r * r < lbm) {
+                r = r_below(lbf);
+                source = 2;
+            }
         }
+        prev_attempts = it;
     }
     if (n_log) *n_log = nl;
     return PADDI_OK;
@@ -431,6 +633,17 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
     ok = ok && cudaMalloc(&ctx->d_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_flatcount, sizeof(int32_t)) == cudaSuccess;
     ok = ok && cudaMallocHost(&ctx->h_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_att1, sizeof(PaddiAttemptDev)) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_one, 2 * sizeof(int32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_nn1, sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&ctx->h_one, 4 * sizeof(int32_t)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&ctx->h_nn1, sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&ctx->h_flatcount, sizeof(int32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_model, sizeof(float) * MLP_NPARAM) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_model_bf16, 2 * MLP_NPARAM) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_feat, sizeof(float) * 16) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_pred, sizeof(float) * 4) == cudaSuccess;
+    ok = ok && cudaMallocHost(&ctx->h_feat, sizeof(float) * 16) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         paddi_ctx_destroy(ctx);
@@ -449,6 +662,17 @@ PADDI_API paddi_status paddi_ctx_destroy(paddi_ctx *ctx)
     dfree(ctx->d_att);
     dfree(ctx->d_res);
     dfree(ctx->d_flatcount);
+    dfree(ctx->d_att1);
+    dfree(ctx->d_one);
+    dfree(ctx->d_nn1);
+    dfree(ctx->d_model);
+    if (ctx->d_model_bf16) cudaFree(ctx->d_model_bf16);
+    dfree(ctx->d_feat);
+    dfree(ctx->d_pred);
+    if (ctx->h_feat) cudaFreeHost(ctx->h_feat);
+    if (ctx->h_flatcount) cudaFreeHost(ctx->h_flatcount);
+    if (ctx->h_one) cudaFreeHost(ctx->h_one);
+    if (ctx->h_nn1) cudaFreeHost(ctx->h_nn1);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -614,5 +838,156 @@ PADDI_API paddi_status paddi_do_pd3(paddi_ctx *ctx, const float *d_T, size_t n, 
         CK(cudaStreamSynchronize(ctx->st));
     }
     if (n_cand) *n_cand = a.res.n_cand;
+    return PADDI_OK;
+}
+
+// ============================================================ learned r model
+PADDI_API paddi_status paddi_r_features(const paddi_discord *out, uint32_t j, uint32_t minL,
+                                        float lb, float flat_frac, uint32_t prev_attempts,
+                                        float *features)
+{
+    if (!features || (j > 0 && !out) || minL < 3) return PADDI_ERR_INVALID_ARG;
+    r_features_impl(out, (int)j, minL, lb, flat_frac, (int)prev_attempts, features);
+    return PADDI_OK;
+}
+
+PADDI_API paddi_status paddi_model_set(paddi_ctx *ctx, const float *params, uint32_t count,
+                                       float margin)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!params || count != MLP_NPARAM || !(margin > 0.f))
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "model parameters: wrong count or margin");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->d_model, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice,
+                       ctx->st));
+    CK(paddi_launch_mlp_to_bf16(ctx->d_model, ctx->d_model_bf16, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->model_ok = true;
+    ctx->model_margin = margin;
+    return PADDI_OK;
+}
+
+namespace {
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+} // namespace
+
+PADDI_API paddi_status paddi_model_grad(paddi_ctx *ctx, const float *X, const float *Y,
+                                        uint32_t n, float tau, const float *params, float *grad,
+                                        float *loss)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!X || !Y || !params || !grad || !loss || n == 0)
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "model_grad: null argument or empty data");
+    CK(cudaSetDevice(ctx->device));
+    DevBuf dX, dY, dP, dG, dL;
+    CK(cudaMalloc(&dX.p, sizeof(float) * MLP_NFEAT * n));
+    CK(cudaMalloc(&dY.p, sizeof(float) * n));
+    CK(cudaMalloc(&dP.p, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&dG.p, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&dL.p, sizeof(float)));
+    cudaStream_t st = ctx->st;
+    CK(cudaMemcpyAsync(dX.p, X, sizeof(float) * MLP_NFEAT * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dY.p, Y, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dP.p, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(dG.p, 0, sizeof(float) * MLP_NPARAM, st));
+    CK(cudaMemsetAsync(dL.p, 0, sizeof(float), st));
+    CK(paddi_launch_mlp_grad((float *)dX.p, (float *)dY.p, (int)n, tau, (float *)dP.p,
+                             (float *)dG.p, (float *)dL.p, ctx->num_sms, st));
+    CK(cudaMemcpyAsync(grad, dG.p, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(loss, dL.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return PADDI_OK;
+}
+
+PADDI_API paddi_status paddi_model_predict(paddi_ctx *ctx, const float *X, uint32_t n,
+                                           const float *params, int32_t bf16, float *Y)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!X || !Y || !params || n == 0)
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "model_predict: null argument or empty data");
+    CK(cudaSetDevice(ctx->device));
+    DevBuf dX, dY, dP, dQ;
+    cudaStream_t st = ctx->st;
+    CK(cudaMalloc(&dX.p, sizeof(float) * MLP_NFEAT * n));
+    CK(cudaMalloc(&dY.p, sizeof(float) * n));
+    CK(cudaMalloc(&dP.p, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&dQ.p, 2 * MLP_NPARAM));
+    CK(cudaMemcpyAsync(dX.p, X, sizeof(float) * MLP_NFEAT * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dP.p, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, st));
+    if (bf16) {
+        CK(paddi_launch_mlp_to_bf16((float *)dP.p, dQ.p, st));
+        CK(paddi_launch_mlp_forward((float *)dX.p, (int)n, dQ.p, true, (float *)dY.p, st));
+    } else {
+        CK(paddi_launch_mlp_forward((float *)dX.p, (int)n, dP.p, false, (float *)dY.p, st));
+    }
+    CK(cudaMemcpyAsync(Y, dY.p, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return PADDI_OK;
+}
+
+PADDI_API paddi_status paddi_model_train(paddi_ctx *ctx, const float *X, const float *Y,
+                                         uint32_t n, float tau, uint32_t epochs, uint32_t batch,
+                                         float lr, uint64_t seed, float *params, float *loss)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!X || !Y || !params || n == 0 || batch == 0 || !(tau > 0.f && tau < 1.f) || !(lr > 0.f))
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "model_train: bad argument");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->st;
+    DevBuf dX, dY, dP, dG, dM, dV, dL;
+    CK(cudaMalloc(&dX.p, sizeof(float) * MLP_NFEAT * n));
+    CK(cudaMalloc(&dY.p, sizeof(float) * n));
+    CK(cudaMalloc(&dP.p, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&dG.p, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&dM.p, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&dV.p, sizeof(float) * MLP_NPARAM));
+    CK(cudaMalloc(&dL.p, sizeof(float) * (epochs ? epochs : 1)));
+    CK(cudaMemcpyAsync(dP.p, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(dG.p, 0, sizeof(float) * MLP_NPARAM, st));
+    CK(cudaMemsetAsync(dM.p, 0, sizeof(float) * MLP_NPARAM, st));
+    CK(cudaMemsetAsync(dV.p, 0, sizeof(float) * MLP_NPARAM, st));
+    CK(cudaMemsetAsync(dL.p, 0, sizeof(float) * (epochs ? epochs : 1), st));
+    std::vector<float> xs((size_t)MLP_NFEAT * n), ys(n);
+    std::vector<uint32_t> perm(n);
+    for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+    uint64_t rng = seed * 6364136223846793005ull + 1442695040888963407ull;
+    int step = 0;
+    for (uint32_t e = 0; e < epochs; ++e) {
+        for (uint32_t i = n - 1; i > 0; --i) { // Fisher-Yates with an LCG
+            rng = rng * 6364136223846793005ull + 1442695040888963407ull;
+            const uint32_t k = (uint32_t)((rng >> 33) % (i + 1));
+            std::swap(perm[i], perm[k]);
+        }
+        CK(cudaStreamSynchronize(st)); // the host buffers are reused each epoch
+        for (uint32_t i = 0; i < n; ++i) {
+            std::memcpy(&xs[(size_t)i * MLP_NFEAT], &X[(size_t)perm[i] * MLP_NFEAT],
+                        sizeof(float) * MLP_NFEAT);
+            ys[i] = Y[perm[i]];
+        }
+        CK(cudaMemcpyAsync(dX.p, xs.data(), sizeof(float) * xs.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dY.p, ys.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+        for (uint32_t b0 = 0; b0 < n; b0 += batch) {
+            const uint32_t bn = std::min(batch, n - b0);
+            CK(paddi_launch_mlp_grad((float *)dX.p + (size_t)b0 * MLP_NFEAT, (float *)dY.p + b0,
+                                     (int)bn, tau, (float *)dP.p, (float *)dG.p,
+                                     (float *)dL.p + e, ctx->num_sms, st));
+            CK(paddi_launch_mlp_adam((float *)dP.p, (float *)dG.p, (float *)dM.p, (float *)dV.p,
+                                     lr, ++step, st));
+        }
+    }
+    CK(cudaMemcpyAsync(params, dP.p, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, st));
+    std::vector<float> lsum(epochs ? epochs : 1);
+    CK(cudaMemcpyAsync(lsum.data(), dL.p, sizeof(float) * lsum.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (loss) {
+        const uint32_t nb = (n + batch - 1) / batch;
+        for (uint32_t e = 0; e < epochs; ++e) loss[e] = lsum[e] / (float)nb;
+    }
     return PADDI_OK;
 }

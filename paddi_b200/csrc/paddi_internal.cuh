@@ -73,7 +73,7 @@ struct PaddiAttemptResult {
 };
 
 #define PADDI_MAX_TOPK 16
-#define PADDI_MAX_RECHECK 1024
+#define PADDI_MAX_RECHECK 1024 /* initial FP64 recheck capacity (grows on demand) */
 
 // ---------------------------------------------------------------- launches
 // All launch wrappers enqueue on `st` and return cudaGetLastError().
@@ -117,9 +117,9 @@ cudaError_t paddi_launch_list_compact(const int32_t *in, const int32_t *in_count
 cudaError_t paddi_launch_finalize(const int32_t *cand, PaddiAttemptDev *att,
                                   const uint32_t *rho_max, const uint8_t *pruned, int32_t m,
                                   float r2, float thr, float guard, float widen, int32_t top_k,
-                                  const uint8_t *flat, int32_t *recheck, int32_t *rc_slot,
-                                  unsigned long long *nn64_ord, PaddiAttemptResult *res,
-                                  cudaStream_t st);
+                                  const uint8_t *flat, int32_t rc_cap, int32_t *recheck,
+                                  int32_t *rc_slot, unsigned long long *nn64_ord,
+                                  PaddiAttemptResult *res, cudaStream_t st);
 
 cudaError_t paddi_launch_recheck(const float *x, const double *mu64, const double *inv64,
                                  const uint8_t *flat, int32_t N, int32_t m,
@@ -144,6 +144,19 @@ cudaError_t paddi_launch_scatter(const int32_t *cand, const PaddiAttemptDev *att
                                  const int32_t *rc_slot, const unsigned long long *nn64_ord,
                                  const uint8_t *flat, int32_t N, int32_t m, float r2,
                                  int32_t *is_cand, float *nnd, cudaStream_t st);
+
+// Learned r predictor (k_mlp.cu).
+#define MLP_NFEAT 12
+#define MLP_HIDDEN 64
+#define MLP_NPARAM (MLP_HIDDEN * MLP_NFEAT + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1)
+cudaError_t paddi_launch_mlp_forward(const float *X, int n, const void *P, bool bf16, float *Y,
+                                     cudaStream_t st);
+cudaError_t paddi_launch_mlp_grad(const float *X, const float *Y, int n, float tau,
+                                  const float *P, float *G, float *loss, int num_sms,
+                                  cudaStream_t st);
+cudaError_t paddi_launch_mlp_adam(float *P, float *G, float *M, float *V, float lr, int step,
+                                  cudaStream_t st);
+cudaError_t paddi_launch_mlp_to_bf16(const float *P, void *Q, cudaStream_t st);
 
 // True when the tcgen05 split refine can run on `device`; longest m it takes.
 bool paddi_umma_supported(int device);

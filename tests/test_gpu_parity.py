@@ -217,3 +217,19 @@ def test_refine_kernels_match_oracle(dist, n, m):
             assert [d.ind for d in got] == [s[0] for s in sel]
             for d, s in zip(got, sel):
                 assert _close(d.dist, s[1])
+
+
+# -------------------------------------------- r policies change work, not results
+@pytest.mark.parametrize("policy", ["bound"])
+def test_r_policy_gives_the_same_discords(policy):
+    rp = {"bound": P.R_BOUND}[policy]
+    x = _series(8192, 5, "palmad")
+    want, _ = O.palmad(x, 40, 60)
+    with P.Context(r_policy=rp) as c:
+        got, log = c.palmad(x, 40, 60)
+    assert [d.ind for d in got] == [w[0] for w in want]
+    for d, w in zip(got, want):
+        assert _close(d.dist, w[1])
+    # a guided attempt uses r^2 below a proven lower bound: it always succeeds
+    guided = [e for e in log if e["r_source"] == 2]
+    assert guided and all(e["found"] for e in guided)
