@@ -306,6 +306,26 @@ def run_paddi(args, world, rank, local):
             "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": 4 * n,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
             "gpu_launches": launches}
+    # the plain form of the headline comparison: FP32 CUDA-core refine with
+    # the reference's MERLIN schedule (same kernels otherwise), one timed run
+    if not args.no_plain_form:
+        with P.Context(device=local, distance_kernel=P.DIST_FP32, r_policy=P.R_MERLIN) as c2:
+            c2.reserve(n, args.maxL)
+            s2 = torch.cuda.ExternalStream(c2.stream)
+            c2.palmad_device(d_x.data_ptr(), n, args.minL, min(args.maxL, args.minL + 8))
+            flush_l2(0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s2)
+            dpl, lpl = c2.palmad_device(d_x.data_ptr(), n, args.minL, args.maxL)
+            e1.record(s2)
+            e1.synchronize()
+            ms_plain = reduce_max(world, e0.elapsed_time(e1))
+        same = [(q.ind, q.dist) for q in dpl] == [(q.ind, q.dist) for q in disc]
+        line["plain_form"] = {"what": "FP32 CUDA-core refine + MERLIN r-schedule",
+                              "ms_per_step": ms_plain, "attempts": len(lpl),
+                              "speedup_of_headline": ms_plain / step_ms,
+                              "same_discords": same}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(x, 1, 0, min(os.cpu_count() or 1, N_SERIES // CPU_SAMPLE_N))
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -321,7 +341,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["paddi", "reference"], default="paddi")
     ap.add_argument("--dist", choices=["auto", "fp32", "bf16", "fp16"], default="auto")
-    ap.add_argument("--r-policy", choices=["merlin", "learned", "bound"], default="merlin")
+    ap.add_argument("--r-policy", choices=["merlin", "learned", "bound"], default="learned")
+    ap.add_argument("--no-plain-form", action="store_true",
+                    help="skip timing the plain FP32 + MERLIN form beside the headline")
     ap.add_argument("--n", type=int, default=N_SERIES)
     ap.add_argument("--minL", type=int, default=MIN_L)
     ap.add_argument("--maxL", type=int, default=MAX_L)

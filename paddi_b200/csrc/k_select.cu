@@ -281,7 +281,14 @@ k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
 // ---------------------------------------------------------------- recheck
 // Exact FP64 nn of the queued windows.  Work items (window, split) are
 // pulled from a counter; each CTA stages the centred candidate window and a
-// slice of the series, one thread per neighbour window.
+// slice of the series (FP64, shifted by its first value); each thread owns 4
+// consecutive neighbour windows and slides a register ring over the slice
+// (one shared load of the slice and one of the candidate per 4 FMAs).
+constexpr int RC_JPT = 4;                    // neighbour windows per thread
+constexpr int RC_SPAN = RC_THREADS * RC_JPT; // neighbour windows per CTA pass
+
+__device__ __forceinline__ int rpad(int d) { return d + (d >> 4); } // 16-lane conflict-free
+
 __global__ void __launch_bounds__(RC_THREADS)
 k_recheck(const float *__restrict__ x, const double *__restrict__ mu64,
           const double *__restrict__ inv64, const uint8_t *__restrict__ flat, int32_t N,
@@ -289,15 +296,16 @@ k_recheck(const float *__restrict__ x, const double *__restrict__ mu64,
           PaddiAttemptDev *att, unsigned long long *nn64_ord, int32_t splits)
 {
     __shared__ double a[RC_MAXM];
-    __shared__ double xs[RC_THREADS + RC_MAXM];
+    __shared__ double xs[RC_SPAN + RC_MAXM + (RC_SPAN + RC_MAXM) / 16 + 8];
     __shared__ double reda[RC_THREADS / 32];
     __shared__ double redm[RC_THREADS / 32];
     __shared__ int s_item;
     const int nr = att->n_recheck;
     const int total = nr * splits;
     const int span = (N + splits - 1) / splits;
+    const int t = threadIdx.x;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&att->recheck_next, 1);
+        if (t == 0) s_item = atomicAdd(&att->recheck_next, 1);
         __syncthreads();
         const int item = s_item;
         __syncthreads();
@@ -307,45 +315,65 @@ k_recheck(const float *__restrict__ x, const double *__restrict__ mu64,
         const double mw = mu64[w], iw = inv64[w];
         const int fw = flat[w];
         double asum = 0.0;
-        for (int k = threadIdx.x; k < m; k += RC_THREADS) {
+        for (int k = t; k < m; k += RC_THREADS) {
             const double v = (double)x[w + k] - mw;
             a[k] = v;
             asum += v;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) asum += __shfl_xor_sync(0xffffffffu, asum, o);
-        if ((threadIdx.x & 31) == 0) reda[threadIdx.x >> 5] = asum;
+        if ((t & 31) == 0) reda[t >> 5] = asum;
         __syncthreads();
         asum = 0.0;
         for (int q = 0; q < RC_THREADS / 32; ++q) asum += reda[q];
         double best = INFINITY;
         const int j_lo = sp * span, j_hi = min(N, j_lo + span);
-        for (int j0 = j_lo; j0 < j_hi; j0 += RC_THREADS) {
+        for (int j0 = j_lo; j0 < j_hi; j0 += RC_SPAN) {
             __syncthreads();
             const double sh = (double)x[j0];
-            for (int p = threadIdx.x; p < RC_THREADS + m - 1; p += RC_THREADS) {
+            for (int p = t; p < RC_SPAN + m + RC_JPT; p += RC_THREADS) {
                 const int g = j0 + p;
-                xs[p] = (g < N + m - 1 ? (double)x[g] : sh) - sh;
+                xs[rpad(p)] = (g < N + m - 1 ? (double)x[g] : sh) - sh;
             }
             __syncthreads();
-            const int j = j0 + threadIdx.x;
-            if (j < j_hi && !overlaps(w, j, m)) {
-                double acc = 0.0;
-                for (int k = 0; k < m; ++k) acc = fma(a[k], xs[threadIdx.x + k], acc);
-                const double cov = acc - (mu64[j] - sh) * asum;
-                double rho;
-                if (fw | flat[j]) rho = (fw & flat[j]) ? 1.0 : 0.0;
-                else rho = cov * iw * inv64[j];
-                double d = 2.0 * m * (1.0 - rho);
-                d = d < 0.0 ? 0.0 : d;
-                best = fmin(best, d);
+            const int q0 = RC_JPT * t;
+            double acc[RC_JPT], ring[RC_JPT];
+#pragma unroll
+            for (int c = 0; c < RC_JPT; ++c) {
+                acc[c] = 0.0;
+                ring[c] = xs[rpad(q0 + c)];
+            }
+            for (int k0 = 0; k0 < m; k0 += RC_JPT) {
+#pragma unroll
+                for (int u = 0; u < RC_JPT; ++u) {
+                    if (k0 + u < m) {
+                        const double ak = a[k0 + u];
+#pragma unroll
+                        for (int c = 0; c < RC_JPT; ++c)
+                            acc[c] = fma(ak, ring[(u + c) & (RC_JPT - 1)], acc[c]);
+                    }
+                    ring[u] = xs[rpad(q0 + k0 + u + RC_JPT)];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < RC_JPT; ++c) {
+                const int j = j0 + q0 + c;
+                if (j < j_hi && !overlaps(w, j, m)) {
+                    const double cov = acc[c] - (mu64[j] - sh) * asum;
+                    double rho;
+                    if (fw | flat[j]) rho = (fw & flat[j]) ? 1.0 : 0.0;
+                    else rho = cov * iw * inv64[j];
+                    double d = 2.0 * m * (1.0 - rho);
+                    d = d < 0.0 ? 0.0 : d;
+                    best = fmin(best, d);
+                }
             }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) best = fmin(best, __shfl_xor_sync(0xffffffffu, best, o));
-        if ((threadIdx.x & 31) == 0) redm[threadIdx.x >> 5] = best;
+        if ((t & 31) == 0) redm[t >> 5] = best;
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (t == 0) {
             double b = INFINITY;
             for (int q = 0; q < RC_THREADS / 32; ++q) b = fmin(b, redm[q]);
             atomicMin(nn64_ord + r, d2ord(b));
