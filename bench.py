@@ -135,13 +135,21 @@ def barrier(world):
 
 
 def reduce_max(world, v: float) -> float:
+    """Max of v over the ranks (the slowest replica sets the step time)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(world: int, pairs_per_replica: float, step_ms_local: float):
+    """Whole-job throughput of `world` replicas: all pairs over the max step time."""
+    step_ms = reduce_max(world, step_ms_local)
+    return world * pairs_per_replica / (step_ms / 1e3), step_ms
 
 
 # ---------------------------------------------------------------- CPU reference
@@ -231,8 +239,7 @@ def run_paddi(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     clocks = clk.summary()
-    step_ms = reduce_max(world, float(np.mean(ms)))
-    value = world * pairs / (step_ms / 1e3)
+    value, step_ms = replica_value(world, pairs, float(np.mean(ms)))
 
     # ---- end to end: host series through paddi_palmad (H2D inside the call)
     e2e_ms = []

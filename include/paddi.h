@@ -158,6 +158,34 @@ paddi_status paddi_palmad_device(paddi_ctx *ctx, const float *d_series, size_t n
                                  uint32_t log_cap, uint32_t *n_log);
 
 /*
+ * PALMAD over many series of uneven length (each at least 2*maxL values).
+ * series[k] (host pointers) has lens[k] values; out receives count*(maxL-minL+1)
+ * discords, out[k*(maxL-minL+1) + i] for series k and length minL+i; status
+ * (optional, count entries) the per-series result.  The series are spread over
+ * `streams` worker contexts (one CUDA stream and host thread each; 0 = 4) so
+ * that their attempt pipelines overlap on the GPU.  Returns the first non-OK
+ * per-series status, or PADDI_OK.  No reference counterpart (the reference runs
+ * one series per invocation).
+ */
+paddi_status paddi_palmad_batched(paddi_ctx *ctx, const float *const *series,
+                                  const size_t *lens, uint32_t count, uint32_t minL,
+                                  uint32_t maxL, uint32_t streams, paddi_discord *out,
+                                  int32_t *status, uint64_t *attempts);
+
+/*
+ * Autotuner: times PALMAD on short probe ranges of this series (three lengths at
+ * the start, middle and end of minL..maxL) for every combination of phase-1
+ * segment length {256, 512, 1024} and phase-1 chunk depth {2, 4, 8}, checks
+ * that all combinations return the same discords, installs the fastest in ctx
+ * and copies the chosen options to *chosen.  ms (optional, 9 entries) receives
+ * the probe time of each combination in the order segment-major.  No
+ * reference counterpart (the reference fixes SEGMENT_N at compile time,
+ * src/parameters.hpp:8-10).
+ */
+paddi_status paddi_autotune(paddi_ctx *ctx, const float *series, size_t n, uint32_t minL,
+                            uint32_t maxL, paddi_opts *chosen, float *ms);
+
+/*
  * Window statistics of length m on the device, FP32 outputs.
  * Replaces compute_statistics (src/preprocessing.cuh:68-76): d_mean[i] and
  * d_std[i] (population) for i < N = n - m + 1, computed from FP64 prefix sums.

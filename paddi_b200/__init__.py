@@ -118,6 +118,11 @@ _SIGS = {
                       C.c_void_p, C.POINTER(C.c_int64), C.c_void_p], C.c_int),
     "paddi_compute_statistics_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                           C.c_uint32, C.c_void_p], C.c_int),
+    "paddi_palmad_batched": ([C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
+                              C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                              C.POINTER(_Discord), C.c_void_p, C.c_void_p], C.c_int),
+    "paddi_autotune": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint32,
+                        C.POINTER(_Opts), C.c_void_p], C.c_int),
     "paddi_r_features": ([C.POINTER(_Discord), C.c_uint32, C.c_uint32, C.c_float, C.c_float,
                           C.c_uint32, C.POINTER(C.c_float)], C.c_int),
     "paddi_model_set": ([C.c_void_p, C.c_void_p, C.c_uint32, C.c_float], C.c_int),
@@ -262,6 +267,33 @@ class Context:
                                        log_cap, C.byref(nl)))
         return ([Discord(out[i].ind, out[i].dist) for i in range(L)],
                 [log[i].as_dict() for i in range(min(nl.value, log_cap))])
+
+    def autotune(self, series, minL: int, maxL: int):
+        """Pick phase-1 segment length and depth on probe lengths of this series."""
+        x = np.ascontiguousarray(series, dtype=np.float32)
+        o = _Opts()
+        ms = np.zeros(9, np.float32)
+        self._check(lib().paddi_autotune(self._h, x.ctypes.data, len(x), minL, maxL,
+                                         C.byref(o), ms.ctypes.data))
+        self.opts = o
+        grid = [(sg, ch) for sg in (256, 512, 1024) for ch in (2, 4, 8)]
+        return {"segment_len": o.segment_len, "phase1_chunks": o.phase1_chunks,
+                "probe_ms": dict(zip(grid, ms.tolist()))}
+
+    def palmad_batched(self, series_list, minL: int, maxL: int, streams: int = 4):
+        """PALMAD over many uneven series; returns (discords per series, attempts)."""
+        arrs = [np.ascontiguousarray(x, dtype=np.float32) for x in series_list]
+        k = len(arrs)
+        ptrs = (C.c_void_p * k)(*[a.ctypes.data for a in arrs])
+        lens = (C.c_size_t * k)(*[len(a) for a in arrs])
+        L = maxL - minL + 1
+        out = (_Discord * max(k * L, 1))()
+        st = np.zeros(max(k, 1), np.int32)
+        att = np.zeros(max(k, 1), np.uint64)
+        self._check(lib().paddi_palmad_batched(self._h, ptrs, lens, k, minL, maxL, streams, out,
+                                               st.ctypes.data, att.ctypes.data))
+        return ([[Discord(out[s * L + i].ind, out[s * L + i].dist) for i in range(L)]
+                 for s in range(k)], att[:k].tolist())
 
     def palmad_device(self, d_series_ptr: int, n: int, minL: int, maxL: int,
                       log_cap: int = 100000):

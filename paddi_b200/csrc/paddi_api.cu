@@ -23,6 +23,8 @@
 #include <cstring>
 #include <string>
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "../../include/paddi.h"
@@ -989,5 +991,142 @@ PADDI_API paddi_status paddi_model_train(paddi_ctx *ctx, const float *X, const f
         const uint32_t nb = (n + batch - 1) / batch;
         for (uint32_t e = 0; e < epochs; ++e) loss[e] = lsum[e] / (float)nb;
     }
+    return PADDI_OK;
+}
+
+// ============================================================ batched PALMAD
+PADDI_API paddi_status paddi_palmad_batched(paddi_ctx *ctx, const float *const *series,
+                                            const size_t *lens, uint32_t count, uint32_t minL,
+                                            uint32_t maxL, uint32_t streams, paddi_discord *out,
+                                            int32_t *status, uint64_t *attempts)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!series || !lens || !out || count == 0)
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "batched: null argument or empty batch");
+    for (uint32_t k = 0; k < count; ++k)
+        if (!series[k] || !valid_lengths(lens[k], minL, maxL))
+            return fail(ctx, PADDI_ERR_INVALID_ARG,
+                        "batched: series " + std::to_string(k) + " invalid or shorter than 2*maxL");
+    const uint32_t L = maxL - minL + 1;
+    int W = streams ? (int)streams : 4;
+    if ((uint32_t)W > count) W = (int)count;
+    // worker contexts share the options (and the model) of ctx
+    std::vector<paddi_ctx *> workers(W, nullptr);
+    paddi_status first_err = PADDI_OK;
+    for (int w = 0; w < W; ++w) {
+        paddi_status s = paddi_ctx_create(&workers[w], &ctx->opts);
+        if (s == PADDI_OK && ctx->model_ok) {
+            std::vector<float> p(MLP_NPARAM);
+            if (cudaMemcpy(p.data(), ctx->d_model, sizeof(float) * MLP_NPARAM,
+                           cudaMemcpyDeviceToHost) != cudaSuccess)
+                s = PADDI_ERR_CUDA;
+            else
+                s = paddi_model_set(workers[w], p.data(), MLP_NPARAM, ctx->model_margin);
+        }
+        if (s != PADDI_OK) {
+            for (auto *c : workers)
+                if (c) paddi_ctx_destroy(c);
+            return fail(ctx, s, "batched: cannot create worker contexts");
+        }
+    }
+    std::atomic<uint32_t> next{0};
+    std::vector<int32_t> st(count, (int32_t)PADDI_OK);
+    std::vector<uint64_t> na(count, 0);
+    std::vector<std::thread> pool;
+    for (int w = 0; w < W; ++w) {
+        pool.emplace_back([&, w]() {
+            paddi_ctx *c = workers[w];
+            cudaSetDevice(c->device);
+            std::vector<paddi_attempt_log> lg(4096);
+            for (uint32_t k = next++; k < count; k = next++) {
+                uint32_t nl = 0;
+                st[k] = (int32_t)paddi_palmad(c, series[k], lens[k], minL, maxL,
+                                              out + (size_t)k * L, lg.data(),
+                                              (uint32_t)lg.size(), &nl);
+                na[k] = nl;
+            }
+        });
+    }
+    for (auto &t : pool) t.join();
+    for (auto *c : workers) paddi_ctx_destroy(c);
+    for (uint32_t k = 0; k < count; ++k) {
+        if (status) status[k] = st[k];
+        if (attempts) attempts[k] = na[k];
+        if (st[k] != PADDI_OK && first_err == PADDI_OK) first_err = (paddi_status)st[k];
+    }
+    if (first_err != PADDI_OK) return fail(ctx, first_err, "batched: a series failed (see status)");
+    return PADDI_OK;
+}
+
+// ================================================================ autotuner
+PADDI_API paddi_status paddi_autotune(paddi_ctx *ctx, const float *series, size_t n,
+                                      uint32_t minL, uint32_t maxL, paddi_opts *chosen,
+                                      float *ms)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!series || !valid_lengths(n, minL, maxL))
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "autotune: invalid series or lengths");
+    CK(cudaSetDevice(ctx->device));
+    paddi_status s = ensure_capacity(ctx, n);
+    if (s != PADDI_OK) return s;
+    CK(cudaMemcpyAsync(ctx->d_x, series, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->st));
+    // probe ranges: 3 consecutive lengths at the start, the middle and the end
+    std::vector<std::pair<uint32_t, uint32_t>> probes;
+    const uint32_t mid = minL + (maxL - minL) / 2;
+    for (uint32_t a : {minL, mid, maxL >= minL + 2 ? maxL - 2 : minL}) {
+        const uint32_t b = std::min(maxL, a + 2);
+        if (probes.empty() || probes.back().first != a) probes.push_back({a, b});
+    }
+    const uint32_t segs[3] = {256, 512, 1024}, chunks[3] = {2, 4, 8};
+    const paddi_opts saved = ctx->opts;
+    std::vector<std::vector<paddi_discord>> ref;
+    float best = FLT_MAX;
+    paddi_opts best_opts = saved;
+    std::vector<paddi_discord> out(3);
+    int idx = 0;
+    for (uint32_t sg : segs)
+        for (uint32_t ch : chunks) {
+            ctx->opts = saved;
+            ctx->opts.segment_len = sg;
+            ctx->opts.phase1_chunks = ch;
+            // one untimed pass (kernel attributes, caches), then the timed one
+            float t_total = 0.f;
+            for (int pass = 0; pass < 2; ++pass) {
+                t_total = 0.f;
+                for (size_t p = 0; p < probes.size(); ++p) {
+                    const uint32_t a = probes[p].first, b = probes[p].second;
+                    out.assign(b - a + 1, paddi_discord{-1, -FLT_MAX});
+                    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+                    s = palmad_impl(ctx, ctx->d_x, n, a, b, out.data(), nullptr, 0, nullptr);
+                    if (s != PADDI_OK) {
+                        ctx->opts = saved;
+                        return s;
+                    }
+                    CK(cudaEventRecord(ctx->ev[7], ctx->st));
+                    CK(cudaEventSynchronize(ctx->ev[7]));
+                    float t = 0.f;
+                    CK(cudaEventElapsedTime(&t, ctx->ev[6], ctx->ev[7]));
+                    t_total += t;
+                    if (pass == 1) {
+                        if (ref.size() <= p) ref.push_back(out);
+                        else
+                            for (size_t q = 0; q < out.size(); ++q)
+                                if (out[q].ind != ref[p][q].ind || out[q].dist != ref[p][q].dist) {
+                                    ctx->opts = saved;
+                                    return fail(ctx, PADDI_ERR_INTERNAL_LIMIT,
+                                                "autotune: configurations disagree");
+                                }
+                    }
+                }
+            }
+            if (ms) ms[idx] = t_total;
+            ++idx;
+            if (t_total < best) {
+                best = t_total;
+                best_opts = ctx->opts;
+            }
+        }
+    ctx->opts = best_opts;
+    if (chosen) *chosen = best_opts;
     return PADDI_OK;
 }

@@ -58,3 +58,10 @@ def test_null_arguments_are_rejected_without_a_device():
     h = C.c_void_p()
     assert L.paddi_ctx_create(C.byref(h), C.byref(o)) in (P.PADDI_ERR_INVALID_ARG,
                                                           P.PADDI_ERR_NO_DEVICE)
+
+
+def test_cli_usage_without_arguments():
+    import subprocess
+    exe = os.path.join(ROOT, "paddi_b200", "paddi-main")
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr

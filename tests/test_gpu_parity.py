@@ -233,3 +233,78 @@ def test_r_policy_gives_the_same_discords(policy):
     # a guided attempt uses r^2 below a proven lower bound: it always succeeds
     guided = [e for e in log if e["r_source"] == 2]
     assert guided and all(e["found"] for e in guided)
+
+
+# ------------------------------------------------------------- batched series
+def test_batched_uneven_series_match_single_runs(ctx):
+    series = [x for x, _ in datagen.batch_series(count=6, seed=3, min_log2=12, max_log2=13,
+                                                 min_anom=32, max_anom=64)]
+    minL, maxL = 32, 40
+    got, att = ctx.palmad_batched(series, minL, maxL, streams=3)
+    for x, g in zip(series, got):
+        want, _ = O.palmad(x, minL, maxL)
+        assert [d.ind for d in g] == [w[0] for w in want]
+        for d, w in zip(g, want):
+            assert _close(d.dist, w[1])
+    assert all(a >= maxL - minL + 1 for a in att)
+
+
+def test_batched_rejects_short_series(ctx):
+    with pytest.raises(P.PaddiError) as e:
+        ctx.palmad_batched([np.zeros(50, np.float32)], 32, 40)
+    assert e.value.status == P.PADDI_ERR_INVALID_ARG
+
+
+# ---------------------------------------------------------------------- CLI
+def test_cli_writes_reference_csv_formats(tmp_path):
+    import os
+    import subprocess
+    x = _series(6000, 8, "palmad")
+    f = tmp_path / "series.txt"
+    np.savetxt(f, x, fmt="%.6f")
+    xr = np.loadtxt(f).astype(np.float32)  # the values the CLI reads
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "paddi_b200", "paddi-main")
+    d, t = tmp_path / "d.csv", tmp_path / "t.csv"
+    r = subprocess.run([exe, str(f), str(len(x)), "40", "46", str(d), str(t)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lines = d.read_text().splitlines()
+    assert lines[0] == "m;top-1 discord idx;top-1 discord nnDist"
+    want, watt = O.palmad(xr, 40, 46)
+    for line, w, m in zip(lines[1:], want, range(40, 47)):
+        mm, ind, dist = line.split(";")
+        assert (int(mm), int(ind)) == (m, w[0])
+        assert abs(float(dist) - w[1]) <= 1e-4 * w[1]
+    tl = t.read_text().splitlines()
+    assert len(tl[0].split(";")) == 14 and len(tl) == 1 + len(watt)
+
+
+# ------------------------------------------------------------------ autotuner
+def test_autotune_picks_a_config_and_keeps_results():
+    x = _series(20000, 12, "palmad")
+    with P.Context() as c:
+        cfg = c.autotune(x, 48, 60)
+        assert cfg["segment_len"] in (256, 512, 1024) and cfg["phase1_chunks"] in (2, 4, 8)
+        assert all(v > 0 for v in cfg["probe_ms"].values())
+        got, _ = c.palmad(x, 48, 60)
+    want, _ = O.palmad(x, 48, 60)
+    assert [d.ind for d in got] == [w[0] for w in want]
+
+
+@pytest.mark.slow
+def test_batched_workload_sample_properties():
+    # a slice of the batched workload (uneven series, L=32..64): the batched
+    # call equals one call per series, and each reported top-1 carries its
+    # exact FP64 nearest-neighbour distance
+    series = [x for x, _ in datagen.batch_series(count=12, seed=2, min_log2=14, max_log2=16)]
+    minL, maxL = 32, 64
+    with P.Context(r_policy=P.R_LEARNED) as c:
+        got, _ = c.palmad_batched(series, minL, maxL, streams=4)
+        one = [c.palmad(x, minL, maxL)[0] for x in series[:3]]
+    assert got[:3] == one
+    rng = np.random.default_rng(0)
+    for x, g in zip(series, got):
+        for i in rng.choice(maxL - minL + 1, 2, replace=False):
+            d, _ = O.window_nn(x, minL + i, g[i].ind)
+            assert abs(g[i].dist - d) <= 1e-5 * d
