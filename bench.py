@@ -40,7 +40,8 @@ import numpy as np  # noqa: E402
 N_SERIES = 1 << 21
 MIN_L, MAX_L = 64, 512
 WORKLOAD = "palmad n=2^21 L=64..512 top-1 (16 planted anomalies, seed 1)"
-CPU_SAMPLE_N = 1 << 15          # points per CPU sample slice
+CPU_SAMPLE_N = 1 << 14          # points per CPU sample slice
+CPU_SLICES_PER_THREAD = 2
 CPU_SAMPLE_LENGTHS = 8          # lengths 64..71
 L2_FLUSH_BYTES = 512 << 20      # > 126 MB L2
 
@@ -153,11 +154,41 @@ def replica_value(world: int, pairs_per_replica: float, step_ms_local: float):
 
 
 # ---------------------------------------------------------------- CPU reference
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def has_flat_run(s, run: int) -> bool:
+    """True when s holds `run` or more consecutive equal values."""
+    eq = np.concatenate([[0], (np.diff(s) == 0).astype(np.int8), [0]])
+    d = np.diff(eq)
+    starts, ends = np.flatnonzero(d == 1), np.flatnonzero(d == -1)
+    return bool(np.any(ends - starts >= run - 1))
+
+
+def cpu_sample_slices(x, count: int):
+    """Up to `count` consecutive 2^14-point slices of the series that hold no
+    flat run of MIN_L points: the reference's FP32 z-normalisation divides by
+    a zero deviation on such windows and its r-schedule then never ends."""
+    out = []
+    for k in range(len(x) // CPU_SAMPLE_N):
+        s = x[k * CPU_SAMPLE_N:(k + 1) * CPU_SAMPLE_N]
+        if not has_flat_run(s, MIN_L):
+            out.append(s)
+        if len(out) == count:
+            break
+    return out
+
+
 def cpu_reference(x, steps: int, warmup: int, threads: int):
     from oracle import oracle as O
     maxl = MIN_L + CPU_SAMPLE_LENGTHS - 1
-    slices = [x[k * CPU_SAMPLE_N:(k + 1) * CPU_SAMPLE_N] for k in range(threads)]
-    pairs = threads * matrix_pairs(CPU_SAMPLE_N, MIN_L, maxl)
+    slices = cpu_sample_slices(x, CPU_SLICES_PER_THREAD * threads)
+    threads = min(threads, len(slices))
+    pairs = len(slices) * matrix_pairs(CPU_SAMPLE_N, MIN_L, maxl)
     for _ in range(warmup):
         O.ref_palmad_many(slices[:1], MIN_L, MIN_L, threads=1)
     t = time.perf_counter()
@@ -165,8 +196,9 @@ def cpu_reference(x, steps: int, warmup: int, threads: int):
         O.ref_palmad_many(slices, MIN_L, maxl, threads=threads)
     el = (time.perf_counter() - t) / steps
     return {"value": pairs / el, "unit": "pairs/s", "cores": threads, "kind": "reference",
-            "sample": f"{threads} slices of {CPU_SAMPLE_N} points of the same series, "
-                      f"lengths {MIN_L}..{maxl}, one slice per thread",
+            "sample": f"{len(slices)} slices of {CPU_SAMPLE_N} points of the same series "
+                      f"(slices without a flat run), lengths {MIN_L}..{maxl}, "
+                      f"{threads} threads taking slices as they free up",
             "s_per_sample": el}
 
 
@@ -175,7 +207,7 @@ def run_reference(args, world, rank):
         return
     from paddi_b200 import datagen
     x, _ = datagen.palmad_series(n=N_SERIES, seed=1)
-    threads = min(os.cpu_count() or 1, N_SERIES // CPU_SAMPLE_N)
+    threads = min(host_threads(), 64)
     cb = cpu_reference(x, args.steps, args.warmup, threads)
     line = {"metric": "PALMAD matrix-equivalent pairs/s (n=2^21, L=64..512, top-1)",
             "value": cb["value"], "unit": "pairs/s", "impl": "reference", "n_gpus": args.gpus,
@@ -191,6 +223,11 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------- GPU arm
+def _progress(rank, msg):
+    if rank == 0:
+        print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def run_paddi(args, world, rank, local):
     import torch
 
@@ -216,10 +253,12 @@ def run_paddi(args, world, rank, local):
         with torch.cuda.stream(st):
             flush.fill_(float(i))
 
+    _progress(rank, "warm-up")
     for i in range(args.warmup):
         flush_l2(i)
         ctx.palmad_device(d_x.data_ptr(), n, args.minL, args.maxL)
     torch.cuda.synchronize()
+    _progress(rank, "timed steps")
 
     # ---- timed: device-resident series, CUDA events on the context's stream
     logs, ms = [], []
@@ -241,6 +280,7 @@ def run_paddi(args, world, rank, local):
     clocks = clk.summary()
     value, step_ms = replica_value(world, pairs, float(np.mean(ms)))
 
+    _progress(rank, "end-to-end steps")
     # ---- end to end: host series through paddi_palmad (H2D inside the call)
     e2e_ms = []
     barrier(world)
@@ -316,6 +356,7 @@ def run_paddi(args, world, rank, local):
     # the plain form of the headline comparison: FP32 CUDA-core refine with
     # the reference's MERLIN schedule (same kernels otherwise), one timed run
     if not args.no_plain_form:
+        _progress(rank, "plain FP32 form")
         with P.Context(device=local, distance_kernel=P.DIST_FP32, r_policy=P.R_MERLIN) as c2:
             c2.reserve(n, args.maxL)
             s2 = torch.cuda.ExternalStream(c2.stream)
@@ -334,7 +375,8 @@ def run_paddi(args, world, rank, local):
                               "speedup_of_headline": ms_plain / step_ms,
                               "same_discords": same}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_reference(x, 1, 0, min(os.cpu_count() or 1, N_SERIES // CPU_SAMPLE_N))
+        _progress(rank, "CPU baseline")
+        cb = cpu_reference(x, 1, 0, min(host_threads(), 64))
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <atomic>
 #include <thread>
 #include <vector>
 
@@ -149,7 +150,7 @@ __attribute__((visibility("default"))) void ref_attempt_at(float *T, int64_t n, 
 }
 
 // Run independent PALMAD jobs on `threads` host threads (one series slice
-// per job).  The reference kernels are pure functions of their arguments,
+// per job, handed out in order to whichever thread is free).  The reference kernels are pure functions of their arguments,
 // so concurrent calls on disjoint buffers are safe.
 __attribute__((visibility("default"))) int64_t ref_palmad_many(float *const *series,
                                                                const int64_t *lens, int32_t jobs,
@@ -160,9 +161,10 @@ __attribute__((visibility("default"))) int64_t ref_palmad_many(float *const *ser
     const int32_t L = maxL - minL + 1;
     std::vector<int64_t> natt(jobs, 0);
     std::vector<std::thread> pool;
+    std::atomic<int32_t> next{0};
     for (int32_t t = 0; t < threads; ++t) {
-        pool.emplace_back([&, t]() {
-            for (int32_t k = t; k < jobs; k += threads)
+        pool.emplace_back([&]() {
+            for (int32_t k; (k = next.fetch_add(1)) < jobs;)
                 natt[k] = ref_palmad(series[k], lens[k], minL, maxL, iter_cap,
                                      out + (size_t)k * L, nullptr, 0);
         });

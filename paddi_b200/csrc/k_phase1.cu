@@ -224,8 +224,7 @@ cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const flo
     if (R < 64 || R > 2048 || (R & 7) || m > P1_MAXM || max_chunks < 1)
         return cudaErrorInvalidValue;
     const size_t smem = paddi_phase1_smem(R, m);
-    cudaError_t e = cudaFuncSetAttribute(k_phase1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = paddi_raise_smem_limit((const void *)k_phase1, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase1, P1_THREADS, smem);

@@ -222,8 +222,7 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
     const int mpad = (m + 7) & ~7;
     const size_t smem = sizeof(float) * ((size_t)mpad * RF_TC + (RF_TW + mpad + 8) +
                                          ((RF_TW + mpad + 8) >> 5) + 4 + 3 * RF_TW) + 16;
-    cudaError_t e = cudaFuncSetAttribute(k_refine_fp32,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = paddi_raise_smem_limit((const void *)k_refine_fp32, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_fp32, RF_THREADS, smem);

@@ -599,8 +599,7 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                  int32_t, int32_t, float, int32_t);
     if (MM == 128) kern = bf16 ? k_refine_umma<true, 128> : k_refine_umma<false, 128>;
     else kern = bf16 ? k_refine_umma<true, 64> : k_refine_umma<false, 64>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = paddi_raise_smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     const int grid = num_sms;
     kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, att, rho_max, pruned,

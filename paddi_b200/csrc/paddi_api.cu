@@ -24,11 +24,28 @@
 #include <string>
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <thread>
 #include <vector>
 
 #include "../../include/paddi.h"
 #include "paddi_internal.cuh"
+
+cudaError_t paddi_raise_smem_limit(const void *func, size_t bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> set;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> g(mu);
+    size_t &cur = set[{dev, func}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
 
 #define PADDI_API extern "C" __attribute__((visibility("default")))
 
@@ -1031,6 +1048,7 @@ PADDI_API paddi_status paddi_palmad_batched(paddi_ctx *ctx, const float *const *
     }
     std::atomic<uint32_t> next{0};
     std::vector<int32_t> st(count, (int32_t)PADDI_OK);
+    std::vector<std::string> errs(count);
     std::vector<uint64_t> na(count, 0);
     std::vector<std::thread> pool;
     for (int w = 0; w < W; ++w) {
@@ -1043,18 +1061,23 @@ PADDI_API paddi_status paddi_palmad_batched(paddi_ctx *ctx, const float *const *
                 st[k] = (int32_t)paddi_palmad(c, series[k], lens[k], minL, maxL,
                                               out + (size_t)k * L, lg.data(),
                                               (uint32_t)lg.size(), &nl);
+                if (st[k] != PADDI_OK) errs[k] = c->err;
                 na[k] = nl;
             }
         });
     }
     for (auto &t : pool) t.join();
     for (auto *c : workers) paddi_ctx_destroy(c);
+    std::string msg;
     for (uint32_t k = 0; k < count; ++k) {
         if (status) status[k] = st[k];
         if (attempts) attempts[k] = na[k];
-        if (st[k] != PADDI_OK && first_err == PADDI_OK) first_err = (paddi_status)st[k];
+        if (st[k] != PADDI_OK && first_err == PADDI_OK) {
+            first_err = (paddi_status)st[k];
+            msg = "batched: series " + std::to_string(k) + ": " + errs[k];
+        }
     }
-    if (first_err != PADDI_OK) return fail(ctx, first_err, "batched: a series failed (see status)");
+    if (first_err != PADDI_OK) return fail(ctx, first_err, msg);
     return PADDI_OK;
 }
 

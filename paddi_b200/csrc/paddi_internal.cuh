@@ -159,5 +159,11 @@ cudaError_t paddi_launch_mlp_adam(float *P, float *G, float *M, float *V, float 
 cudaError_t paddi_launch_mlp_to_bf16(const float *P, void *Q, cudaStream_t st);
 
 // True when the tcgen05 split refine can run on `device`; longest m it takes.
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device.  The limit is a process-wide attribute of the function, so
+// host threads that launch the same kernel with different sizes could lower
+// it under one another; here it only grows, under a lock.
+cudaError_t paddi_raise_smem_limit(const void *func, size_t bytes);
+
 bool paddi_umma_supported(int device);
 int paddi_umma_max_m();
