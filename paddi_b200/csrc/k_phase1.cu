@@ -11,80 +11,127 @@
 //   * a persistent grid pulls (segment, chunk) tasks chunk-major from a
 //     global counter, so every segment's nearest chunk is done before any
 //     segment continues, and segments whose rows are all pruned drop out;
-//   * a task is R rows x 1024 diagonals; each thread owns 8 consecutive
-//     diagonals and walks all R rows with the centred covariance update
+//   * a task is R rows x 1024 diagonals; each thread owns the 4 diagonals
+//     4t..4t+3 and their partners 512 further on, and walks all R rows with
+//     the centred covariance update
 //         cov(i+1, j+1) = cov(i, j) + df_i dg_j + df_j dg_i
-//     (no shared-memory traffic per pair: the 8 column operands rotate
-//     through a register ring, one 16-byte load per step);
+//     on (diagonal, partner) pairs with packed f32x2 FMAs; the column
+//     operands come pair-packed from shared memory ((col q, col q+512) per
+//     entry, XOR-swizzled so the stride-4 ring loads are conflict-free) and
+//     rotate through a 4-entry register ring, one entry per row step;
 //   * the starting covariances of the 1024 diagonals are m-term dot products
 //     of the centred first row window with the shifted series;
-//   * pruned rows are found with one warp ballot per step, pruned columns
-//     through shared-memory byte flags; both are flushed as byte stores of 0
-//     to the global alive[] array (idempotent, so no atomics).
+//   * hits are tracked as running maxima of rho (per row step over the
+//     thread's 8 diagonals; per column over the rows that touch it), and only
+//     the maxima are compared with the threshold: a row is pruned through one
+//     warp ballot per step, a column when it leaves the thread's ring; both
+//     go to shared-memory byte flags and are flushed as byte stores of 0 to
+//     the global alive[] array (idempotent, so no atomics).
 // Pruning uses rho > thr_prune where thr_prune = 1 - r^2/(2m) + guard, so a
 // window is pruned only when its FP32 correlation clears the threshold by
 // more than the rounding bound; everything else stays a candidate and is
 // settled by the refine and the FP64 recheck.
+#include <algorithm>
+
 #include "paddi_internal.cuh"
 
 namespace {
 
 constexpr int P1_THREADS = 128;
-constexpr int P1_DPT = 8;                      // diagonals per thread
-constexpr int P1_D = P1_THREADS * P1_DPT;      // diagonals per chunk
+constexpr int P1_GPT = 4;                     // diagonal pairs per thread
+constexpr int P1_H = P1_THREADS * P1_GPT;     // partner offset (512)
+constexpr int P1_D = 2 * P1_H;                // diagonals per chunk
 constexpr int P1_MAXM = 1024;
 
-__device__ __forceinline__ int cpad(int q) { return q + (q >> 3); } // float4 index, conflict-free stride-8
-__device__ __forceinline__ int xpad(int p) { return p + (p >> 5); } // float index, conflict-free stride-8
+// pair-packed column arrays: stride-4 float4 / float2 loads conflict-free
+__host__ __device__ __forceinline__ int csw(int q) { return q ^ ((q >> 2) & 15); }
+__host__ __device__ __forceinline__ int xpad(int p) { return p + (p >> 5); } // stride-4 floats
+__host__ __device__ __forceinline__ int p1_ncp(int R) { return (R + P1_H + 63) & ~63; }
+
+// max(a, b, c) in one instruction (sm_100 three-input form)
+__device__ __forceinline__ float fmax3(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
 
 struct P1Smem {
-    float4 *roww;  // R
-    float4 *colw;  // cpad(R + D)
-    float *xa;     // mpad
-    float *xb;     // xpad(D + mpad + 8)
+    float4 *roww;     // R
+    float2 *colz;     // ncp: (inv_q, inv_q+H)
+    float2 *colw;     // ncp: (flat term q, q+H)
+    float4 *colxy;    // ncp: (df_q, df_q+H, dg_q, dg_q+H); aliases xa / xb
+    float *xa;        // mpad
+    float *xb;        // xpad(D + mpad + 8)
     uint8_t *colflag; // R + D
     uint8_t *rowflag; // R
 };
 
 template <bool FLATS, bool BOUND>
-__device__ __forceinline__ void p1_walk(const P1Smem &S, float (&cov)[P1_DPT], int R, int rows,
+__device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], int R, int rows,
                                         int lim, float thr, int t)
 {
     const int lane = threadIdx.x & 31;
-    float4 ring[P1_DPT];
+    const int c0 = P1_GPT * t;
+    float4 rxy[4];
+    float2 rz[4], rw[4];
 #pragma unroll
-    for (int k = 0; k < P1_DPT; ++k) ring[k] = S.colw[cpad(8 * t + k)];
-    uint32_t colbits = 0;
-    for (int s0 = 0; s0 < R; s0 += 8) {
+    for (int k = 0; k < 4; ++k) {
+        rxy[k] = S.colxy[csw(c0 + k)];
+        rz[k] = S.colz[csw(c0 + k)];
+        if (FLATS) rw[k] = S.colw[csw(c0 + k)];
+        else rw[k] = make_float2(0.f, 0.f);
+    }
+    float cmA[4], cmB[4];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+    for (int k = 0; k < 4; ++k) cmA[k] = cmB[k] = -INFINITY;
+    for (int s0 = 0; s0 < R; s0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
             const int s = s0 + u;
             const float4 ri = S.roww[s];
-            bool rh = false;
+            const float2 rix = make_float2(ri.x, ri.x), riy = make_float2(ri.y, ri.y);
+            const float2 riz = make_float2(ri.z, ri.z), riw = make_float2(ri.w, ri.w);
+            float rmax = -INFINITY;
 #pragma unroll
-            for (int k = 0; k < P1_DPT; ++k) {
-                const float4 cj = ring[(u + k) & 7];
-                float rho;
-                if (FLATS) rho = fmaf(cov[k] * ri.z, cj.z, ri.w * cj.w);
-                else rho = cov[k] * ri.z * cj.z;
-                bool h = rho > thr;
-                if (BOUND) h = h && (s < rows) && (s + 8 * t + k < lim);
-                rh |= h;
-                colbits |= (uint32_t)h << ((u + k) & 7);
-                cov[k] = fmaf(ri.x, cj.y, fmaf(cj.x, ri.y, cov[k]));
+            for (int k = 0; k < P1_GPT; ++k) {
+                const int sl = (u + k) & 3;
+                const float2 cx = make_float2(rxy[sl].x, rxy[sl].y);
+                const float2 cy = make_float2(rxy[sl].z, rxy[sl].w);
+                float2 rho;
+                if (FLATS) rho = __ffma2_rn(__fmul2_rn(cov[k], riz), rz[sl], __fmul2_rn(riw, rw[sl]));
+                else rho = __fmul2_rn(__fmul2_rn(cov[k], riz), rz[sl]);
+                if (BOUND) {
+                    const int q = s + c0 + k;
+                    if (s >= rows || q >= lim) rho.x = -INFINITY;
+                    if (s >= rows || q + P1_H >= lim) rho.y = -INFINITY;
+                }
+                rmax = fmax3(rmax, rho.x, rho.y);
+                cmA[sl] = fmaxf(cmA[sl], rho.x);
+                cmB[sl] = fmaxf(cmB[sl], rho.y);
+                cov[k] = __ffma2_rn(rix, cy, __ffma2_rn(cx, riy, cov[k]));
             }
-            if (__ballot_sync(0xffffffffu, rh) && lane == 0) S.rowflag[s] = 1;
-            if ((colbits >> u) & 1u) S.colflag[s + 8 * t] = 1;
-            colbits &= ~(1u << u);
-            ring[u] = S.colw[cpad(s + 8 * t + 8)];
+            if (__ballot_sync(0xffffffffu, rmax > thr) && lane == 0) S.rowflag[s] = 1;
+            // columns s + c0 and s + c0 + H leave the ring: no later row touches them
+            if (cmA[u] > thr) S.colflag[s + c0] = 1;
+            if (cmB[u] > thr) S.colflag[s + c0 + P1_H] = 1;
+            cmA[u] = -INFINITY;
+            cmB[u] = -INFINITY;
+            const int qn = csw(s + c0 + 4);
+            rxy[u] = S.colxy[qn];
+            rz[u] = S.colz[qn];
+            if (FLATS) rw[u] = S.colw[qn];
         }
     }
+    // columns R + c0 + e (e < 3) were touched by the last rows only
 #pragma unroll
-    for (int k = 0; k < P1_DPT; ++k)
-        if ((colbits >> k) & 1u) S.colflag[R + 8 * t + k] = 1;
+    for (int e = 0; e < 3; ++e) {
+        if (cmA[e] > thr) S.colflag[R + c0 + e] = 1;
+        if (cmB[e] > thr) S.colflag[R + c0 + e + P1_H] = 1;
+    }
 }
 
-__global__ void __launch_bounds__(P1_THREADS)
+__global__ void __launch_bounds__(P1_THREADS, 5)
 k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const float *__restrict__ mu,
          uint8_t *alive, int32_t N, int32_t m, int32_t R, int32_t max_chunks, float thr,
          const int32_t *__restrict__ flat_count, int32_t *task_counter)
@@ -92,17 +139,23 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
     const bool flats = *flat_count > 0;
     extern __shared__ __align__(16) unsigned char p1_smem[];
     const int mpad = (m + 7) & ~7;
+    const int ncp = p1_ncp(R);
     P1Smem S;
     S.roww = reinterpret_cast<float4 *>(p1_smem);
-    S.colw = S.roww + R;
-    S.xa = reinterpret_cast<float *>(S.colw + cpad(R + P1_D) + 1);
+    S.colz = reinterpret_cast<float2 *>(S.roww + R);
+    S.colw = S.colz + ncp;
+    S.colxy = reinterpret_cast<float4 *>(S.colw + ncp);
+    S.xa = reinterpret_cast<float *>(S.colxy);
     S.xb = S.xa + mpad;
-    S.colflag = reinterpret_cast<uint8_t *>(S.xb + xpad(P1_D + mpad + 8) + 1);
+    const size_t ubytes = max((size_t)16 * ncp,
+                              (size_t)4 * (mpad + xpad(P1_D + mpad + 8) + 1));
+    S.colflag = reinterpret_cast<uint8_t *>(S.colxy) + ((ubytes + 15) & ~(size_t)15);
     S.rowflag = S.colflag + R + P1_D;
     __shared__ int s_task;
     __shared__ float s_red[P1_THREADS / 32];
 
     const int t = threadIdx.x;
+    const int c0 = P1_GPT * t;
     const int nseg = (N + R - 1) / R;
     const int total = nseg * max_chunks;
     for (;;) {
@@ -124,15 +177,18 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
             any = __syncthreads_or(any);
             if (!any) continue;
         }
-        // ---- stage rows, columns, and the series slices for the start dots
+        // ---- stage rows, flags, the (inv, flat) column pairs and the series
+        //      slices for the start dots
         for (int s = t; s < R; s += P1_THREADS) {
             S.roww[s] = wst[i0 + s]; // zero beyond N (padded tail)
             S.rowflag[s] = 0;
         }
         const int cbase = i0 + d0;
-        for (int q = t; q < R + P1_D; q += P1_THREADS) {
-            S.colw[cpad(q)] = wst[cbase + q];
-            S.colflag[q] = 0;
+        for (int q = t; q < R + P1_D; q += P1_THREADS) S.colflag[q] = 0;
+        for (int q = t; q < R + P1_H; q += P1_THREADS) {
+            const float4 a = wst[cbase + q], b = wst[cbase + q + P1_H];
+            S.colz[csw(q)] = make_float2(a.z, b.z);
+            S.colw[csw(q)] = make_float2(a.w, b.w);
         }
         const float mu0 = mu[i0];
         float zs = 0.f;
@@ -155,30 +211,44 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
 #pragma unroll
         for (int w = 0; w < P1_THREADS / 32; ++w) zsum += s_red[w];
 
-        // ---- starting covariances of diagonals d0 + 8t + k at row i0
-        float cov[P1_DPT];
-#pragma unroll
-        for (int k = 0; k < P1_DPT; ++k) cov[k] = 0.f;
+        // ---- starting covariances of diagonals d0 + c0 + k and d0 + c0 + k + H
+        float2 cov[P1_GPT];
         {
-            float b[8];
+            float accA[P1_GPT], accB[P1_GPT], bA[4], bB[4];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) b[k] = S.xb[xpad(8 * t + k)];
-            for (int q0 = 0; q0 < mpad; q0 += 8) {
+            for (int k = 0; k < P1_GPT; ++k) {
+                accA[k] = accB[k] = 0.f;
+                bA[k] = S.xb[xpad(c0 + k)];
+                bB[k] = S.xb[xpad(c0 + P1_H + k)];
+            }
+            for (int q0 = 0; q0 < mpad; q0 += 4) {
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
+                for (int u = 0; u < 4; ++u) {
                     const float a = S.xa[q0 + u];
 #pragma unroll
-                    for (int k = 0; k < P1_DPT; ++k) cov[k] = fmaf(a, b[(u + k) & 7], cov[k]);
-                    b[u] = S.xb[xpad(8 * t + q0 + u + 8)];
+                    for (int k = 0; k < P1_GPT; ++k) {
+                        accA[k] = fmaf(a, bA[(u + k) & 3], accA[k]);
+                        accB[k] = fmaf(a, bB[(u + k) & 3], accB[k]);
+                    }
+                    bA[u] = S.xb[xpad(c0 + q0 + u + 4)];
+                    bB[u] = S.xb[xpad(c0 + P1_H + q0 + u + 4)];
                 }
             }
-        }
 #pragma unroll
-        for (int k = 0; k < P1_DPT; ++k) {
-            const int j = cbase + 8 * t + k;
-            const float muj = j < N ? mu[j] : shift;
-            cov[k] = fmaf(-(muj - shift), zsum, cov[k]);
+            for (int k = 0; k < P1_GPT; ++k) {
+                const int ja = cbase + c0 + k, jb = ja + P1_H;
+                const float mua = ja < N ? mu[ja] : shift;
+                const float mub = jb < N ? mu[jb] : shift;
+                cov[k] = make_float2(fmaf(-(mua - shift), zsum, accA[k]),
+                                     fmaf(-(mub - shift), zsum, accB[k]));
+            }
         }
+        __syncthreads(); // xa / xb are overwritten by the (df, dg) column pairs
+        for (int q = t; q < R + P1_H; q += P1_THREADS) {
+            const float4 a = wst[cbase + q], b = wst[cbase + q + P1_H];
+            S.colxy[csw(q)] = make_float4(a.x, b.x, a.y, b.y);
+        }
+        __syncthreads();
         // ---- walk the R rows
         const int lim = N - cbase; // column q is a window iff q < lim
         const bool bound = (rows < R) || (R + P1_D > lim);
@@ -204,14 +274,13 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
 size_t paddi_phase1_smem(int R, int m)
 {
     const int mpad = (m + 7) & ~7;
-    auto cpadh = [](int q) { return q + (q >> 3); };
-    auto xpadh = [](int p) { return p + (p >> 5); };
-    size_t b = 0;
-    b += sizeof(float4) * (size_t)R;
-    b += sizeof(float4) * (size_t)(cpadh(R + P1_D) + 1);
-    b += sizeof(float) * (size_t)mpad;
-    b += sizeof(float) * (size_t)(xpadh(P1_D + mpad + 8) + 1);
-    b += (size_t)(R + P1_D) + (size_t)R;
+    const int ncp = p1_ncp(R);
+    size_t b = sizeof(float4) * (size_t)R;   // roww
+    b += 2 * sizeof(float2) * (size_t)ncp;   // colz, colw
+    const size_t ubytes = std::max((size_t)16 * ncp,
+                                   (size_t)4 * (mpad + xpad(P1_D + mpad + 8) + 1));
+    b += (ubytes + 15) & ~(size_t)15;        // colxy / xa + xb
+    b += (size_t)(R + P1_D) + (size_t)R;     // flags
     return (b + 15) & ~(size_t)15;
 }
 

@@ -279,30 +279,37 @@ k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
 }
 
 // ---------------------------------------------------------------- recheck
-// Exact FP64 nn of the queued windows.  Work items (window, split) are
-// pulled from a counter; each CTA stages the centred candidate window and a
-// slice of the series (FP64, shifted by its first value); each thread owns 4
+// Exact FP64 nn of the queued windows.  The neighbour range is cut into
+// blocks of RC_SPAN windows; a work item is (queued window, run of `per`
+// consecutive blocks), with `per` chosen on the device from the queue length
+// so that the items fill the grid about four times over even for one queued
+// window.  Each CTA stages the centred candidate window and a slice of the
+// series (FP64, shifted by its first value); each thread owns RC_JPT
 // consecutive neighbour windows and slides a register ring over the slice
-// (one shared load of the slice and one of the candidate per 4 FMAs).
-constexpr int RC_JPT = 4;                    // neighbour windows per thread
-constexpr int RC_SPAN = RC_THREADS * RC_JPT; // neighbour windows per CTA pass
+// (per step: one shared load of the slice, one broadcast of the candidate,
+// RC_JPT FP64 FMAs).
+constexpr int RC_JPT = 8;                    // neighbour windows per thread
+constexpr int RC_SPAN = RC_THREADS * RC_JPT; // neighbour windows per block
 
-__device__ __forceinline__ int rpad(int d) { return d + (d >> 4); } // 16-lane conflict-free
+__device__ __forceinline__ int rpad(int d) { return d + (d >> 4); } // conflict-free at stride 8
 
 __global__ void __launch_bounds__(RC_THREADS)
 k_recheck(const float *__restrict__ x, const double *__restrict__ mu64,
           const double *__restrict__ inv64, const uint8_t *__restrict__ flat, int32_t N,
           int32_t m, const int32_t *__restrict__ cand, const int32_t *__restrict__ recheck,
-          PaddiAttemptDev *att, unsigned long long *nn64_ord, int32_t splits)
+          PaddiAttemptDev *att, unsigned long long *nn64_ord)
 {
     __shared__ double a[RC_MAXM];
-    __shared__ double xs[RC_SPAN + RC_MAXM + (RC_SPAN + RC_MAXM) / 16 + 8];
+    __shared__ double xs[RC_SPAN + RC_MAXM + (RC_SPAN + RC_MAXM) / 16 + 16];
     __shared__ double reda[RC_THREADS / 32];
     __shared__ double redm[RC_THREADS / 32];
     __shared__ int s_item;
     const int nr = att->n_recheck;
-    const int total = nr * splits;
-    const int span = (N + splits - 1) / splits;
+    const int nblk = (N + RC_SPAN - 1) / RC_SPAN;
+    const long long want = 4ll * gridDim.x;
+    const int per = (int)max(1ll, ((long long)nr * nblk) / want); // blocks per item
+    const int ipc = (nblk + per - 1) / per;                        // items per queued window
+    const long long total = (long long)nr * ipc;
     const int t = threadIdx.x;
     for (;;) {
         if (t == 0) s_item = atomicAdd(&att->recheck_next, 1);
@@ -327,7 +334,8 @@ k_recheck(const float *__restrict__ x, const double *__restrict__ mu64,
         asum = 0.0;
         for (int q = 0; q < RC_THREADS / 32; ++q) asum += reda[q];
         double best = INFINITY;
-        const int j_lo = sp * span, j_hi = min(N, j_lo + span);
+        const int j_lo = sp * per * RC_SPAN;
+        const int j_hi = (int)min((long long)N, (long long)j_lo + (long long)per * RC_SPAN);
         for (int j0 = j_lo; j0 < j_hi; j0 += RC_SPAN) {
             __syncthreads();
             const double sh = (double)x[j0];
@@ -551,11 +559,11 @@ cudaError_t paddi_launch_recheck(const float *x, const double *mu64, const doubl
                                  const uint8_t *flat, int32_t N, int32_t m,
                                  const int32_t *cand, const int32_t *recheck,
                                  PaddiAttemptDev *att, unsigned long long *nn64_ord,
-                                 int32_t num_sms, int32_t splits, cudaStream_t st)
+                                 int32_t num_sms, cudaStream_t st)
 {
     if (m > RC_MAXM) return cudaErrorInvalidValue;
     k_recheck<<<num_sms * 4, RC_THREADS, 0, st>>>(x, mu64, inv64, flat, N, m, cand, recheck, att,
-                                                 nn64_ord, splits);
+                                                 nn64_ord);
     return cudaGetLastError();
 }
 

@@ -273,8 +273,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
                                  guard, widen, top_k, ctx->d_flat, ctx->rc_cap, ctx->d_recheck,
                                  ctx->d_rcslot, ctx->d_nn64, ctx->d_res, st));
         CK(paddi_launch_recheck(x, ctx->d_mu64, ctx->d_inv64, ctx->d_flat, N, m, ctx->d_cand,
-                                ctx->d_recheck, ctx->d_att, ctx->d_nn64, ctx->num_sms,
-                                /*splits=*/ctx->num_sms, st));
+                                ctx->d_recheck, ctx->d_att, ctx->d_nn64, ctx->num_sms, st));
         CK(paddi_launch_select(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned,
                                ctx->d_recheck, ctx->d_rcslot, ctx->d_nn64, m, r2, thr, guard,
                                top_k, ctx->d_flat, ctx->d_res, st));
@@ -377,8 +376,7 @@ paddi_status window_nn64(paddi_ctx *ctx, const float *x, size_t n, int m, int w,
     CK(cudaMemcpyAsync(ctx->d_att1, &a1, sizeof(a1), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ctx->d_nn1, 0xff, sizeof(unsigned long long), st)); // +inf image
     CK(paddi_launch_recheck(x, ctx->d_mu64, ctx->d_inv64, ctx->d_flat, N, m, ctx->d_one,
-                            ctx->d_one + 1, ctx->d_att1, ctx->d_nn1, ctx->num_sms,
-                            ctx->num_sms, st));
+                            ctx->d_one + 1, ctx->d_att1, ctx->d_nn1, ctx->num_sms, st));
     CK(cudaMemcpyAsync(ctx->h_nn1, ctx->d_nn1, sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -570,13 +568,21 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
             ++nl;
             first = false;
             if (out[j].dist >= 0) break;
-            // no discord: lower r as MERLIN does; the guided policies never go below
-            // the bound, where a discord is certain
+            // no discord: MERLIN lowers r by its own schedule (src/main.cu:216-233).
+            // The guided policies lower r^2 by at least 15% (30% from the second
+            // miss on): after a sudden drop of the top-1 distance (a flat run that
+            // ends) MERLIN's decrement S is tiny and would take dozens of attempts.
+            // They never go below the bound, where a discord is certain.
             r = merlin_lower(r, j, S);
             source = 0;
-            if (policy != PADDI_R_MERLIN && lbm > 0.f && r * r < lbm) {
-                r = r_below(lbf);
-                source = 2;
+            if (policy != PADDI_R_MERLIN) {
+                const float q = it == 1 ? 0.85f : 0.7f;
+                const float rg = r2 > 0.f ? r_below(q * r2) : 0.f;
+                if (rg < r) r = rg;
+                if (lbm > 0.f && r * r < lbm) {
+                    r = r_below(lbf);
+                    source = 2;
+                }
             }
         }
         prev_attempts = it;

@@ -125,7 +125,7 @@ cudaError_t paddi_launch_recheck(const float *x, const double *mu64, const doubl
                                  const uint8_t *flat, int32_t N, int32_t m,
                                  const int32_t *cand, const int32_t *recheck,
                                  PaddiAttemptDev *att, unsigned long long *nn64_ord,
-                                 int32_t num_sms, int32_t splits, cudaStream_t st);
+                                 int32_t num_sms, cudaStream_t st);
 
 cudaError_t paddi_launch_select(const int32_t *cand, PaddiAttemptDev *att,
                                 const uint32_t *rho_max, const uint8_t *pruned,
