@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <algorithm>
@@ -55,6 +56,11 @@ struct paddi_ctx {
     int num_sms = 0;
     cudaStream_t st = nullptr;
     cudaEvent_t ev[8] = {};
+    // PADDI_TRACE=1 in the environment: one stderr line per attempt with the
+    // live-candidate count and the time of every refine round
+    bool trace = false;
+    cudaEvent_t tev[9] = {};
+    int32_t *d_trace = nullptr, *h_trace = nullptr;
     std::string err;
     size_t cap_n = 0; // series capacity (values)
     int32_t rc_cap = 0; // FP64 recheck capacity (windows)
@@ -219,7 +225,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     R = (R + 7) & ~7;
     if (R < 64) R = 64;
     if (R > 1024) R = 1024;
-    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 4;
+    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 2;
     cudaStream_t st = ctx->st;
     CK(cudaEventRecord(ctx->ev[0], st));
     CK(cudaMemsetAsync(ctx->d_alive, 1, (size_t)N, st));
@@ -232,19 +238,26 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     CK(paddi_launch_compact(ctx->d_alive, N, ctx->d_cand, ctx->d_rho, ctx->d_pruned,
                             ctx->d_rcslot, ctx->d_att, st));
     ++launches;
-    // refine rounds over geometrically growing window ranges; survivors are
-    // re-compacted between rounds so every tile is dense with live candidates
+    // refine rounds over growing window ranges; survivors are re-compacted
+    // between rounds so every tile is dense with live candidates
     CK(paddi_launch_list_init(ctx->d_att, ctx->d_list[0], &ctx->d_att->list_count[0], st));
     ++launches;
     const bool umma = kernel != PADDI_DIST_FP32;
     out->kernel = kernel;
-    const int nrounds = N >= (1 << 16) ? 8 : 1;
+    // range edges N/32, N/8, N/4, N/2, N: the first rounds prune only a small
+    // share each, so they are merged into one (fewer launches, longer items)
+    constexpr int kShifts[4] = {5, 3, 2, 1};
+    const int nrounds = N >= (1 << 16) ? 5 : 1;
     int jb = 0;
     for (int rd = 0; rd < nrounds; ++rd) {
-        // range sizes N/128, N/128, N/64, ..., N/2 (the last round takes the rest)
-        int je = rd == nrounds - 1 ? N : jb + (int)((int64_t)N >> (nrounds - (rd == 0 ? 1 : rd)));
+        int je = rd == nrounds - 1 ? N : (int)((int64_t)N >> kShifts[rd]);
         if (je > N) je = N;
         const int a = rd & 1, b = a ^ 1;
+        if (ctx->trace) {
+            CK(cudaEventRecord(ctx->tev[rd], st));
+            CK(cudaMemcpyAsync(ctx->d_trace + rd, &ctx->d_att->list_count[a], sizeof(int32_t),
+                               cudaMemcpyDeviceToDevice, st));
+        }
         CK(cudaMemsetAsync(&ctx->d_att->work_next, 0, sizeof(int32_t), st));
         if (umma)
             CK(paddi_launch_refine_umma(kernel == PADDI_DIST_SPLIT_BF16, x, ctx->d_wst, ctx->d_mu,
@@ -267,6 +280,11 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         jb = je;
     }
     CK(cudaEventRecord(ctx->ev[2], st));
+    if (ctx->trace) {
+        CK(cudaEventRecord(ctx->tev[nrounds], st));
+        CK(cudaMemcpyAsync(ctx->h_trace, ctx->d_trace, sizeof(int32_t) * nrounds,
+                           cudaMemcpyDeviceToHost, st));
+    }
     float widen = 2.f;
     for (int pass = 0; pass < 6; ++pass) {
         CK(paddi_launch_finalize(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned, m, r2, thr,
@@ -314,6 +332,16 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT, "top-k selection did not settle");
     out->res = *ctx->h_res;
     out->launches = launches;
+    if (ctx->trace) {
+        std::string line = "paddi-trace m=" + std::to_string(m) + " r2=" + std::to_string(r2) +
+                           " p1=" + std::to_string(ctx->h_res->n_p1) + " rounds:";
+        for (int rd = 0; rd < nrounds; ++rd) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ctx->tev[rd], ctx->tev[rd + 1]));
+            line += " " + std::to_string(ctx->h_trace[rd]) + "/" + std::to_string(ms);
+        }
+        std::fprintf(stderr, "%s disc=%lld\n", line.c_str(), (long long)ctx->h_res->n_disc);
+    }
     CK(cudaEventElapsedTime(&out->ms_phase1, ctx->ev[0], ctx->ev[1]));
     CK(cudaEventElapsedTime(&out->ms_refine, ctx->ev[1], ctx->ev[2]));
     CK(cudaEventElapsedTime(&out->ms_select, ctx->ev[2], ctx->ev[3]));
@@ -611,7 +639,7 @@ PADDI_API void paddi_opts_default(paddi_opts *o)
     o->distance_kernel = PADDI_DIST_AUTO;
     o->r_policy = PADDI_R_MERLIN;
     o->segment_len = 512;
-    o->phase1_chunks = 4;
+    o->phase1_chunks = 2;
     o->iter_cap = 200;
     o->guard = 0.f;
 }
@@ -654,6 +682,15 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
     }
     bool ok = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) == cudaSuccess;
     for (auto &e : ctx->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+    {
+        const char *tr = std::getenv("PADDI_TRACE");
+        ctx->trace = tr && tr[0] && tr[0] != '0';
+    }
+    if (ctx->trace) {
+        for (auto &e : ctx->tev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+        ok = ok && cudaMalloc(&ctx->d_trace, 8 * sizeof(int32_t)) == cudaSuccess;
+        ok = ok && cudaMallocHost(&ctx->h_trace, 8 * sizeof(int32_t)) == cudaSuccess;
+    }
     ok = ok && cudaMalloc(&ctx->d_att, sizeof(PaddiAttemptDev)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_flatcount, sizeof(int32_t)) == cudaSuccess;
@@ -701,6 +738,10 @@ PADDI_API paddi_status paddi_ctx_destroy(paddi_ctx *ctx)
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    for (auto &e : ctx->tev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->d_trace) cudaFree(ctx->d_trace);
+    if (ctx->h_trace) cudaFreeHost(ctx->h_trace);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
     return PADDI_OK;
@@ -1106,7 +1147,7 @@ PADDI_API paddi_status paddi_autotune(paddi_ctx *ctx, const float *series, size_
         const uint32_t b = std::min(maxL, a + 2);
         if (probes.empty() || probes.back().first != a) probes.push_back({a, b});
     }
-    const uint32_t segs[3] = {256, 512, 1024}, chunks[3] = {2, 4, 8};
+    const uint32_t segs[3] = {256, 512, 1024}, chunks[3] = {1, 2, 4};
     const paddi_opts saved = ctx->opts;
     std::vector<std::vector<paddi_discord>> ref;
     float best = FLT_MAX;
