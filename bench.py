@@ -44,6 +44,10 @@ CPU_SAMPLE_N = 1 << 14          # points per CPU sample slice
 CPU_SLICES_PER_THREAD = 2
 CPU_SAMPLE_LENGTHS = 8          # lengths 64..71
 L2_FLUSH_BYTES = 512 << 20      # > 126 MB L2
+# DRAM bytes (read + write) of one k_refine_umma launch from an ncu capture:
+# the last refine round (windows N/2..N) of an m=300 attempt on this series
+REFINE_TRAFFIC_BYTES = 25230336 + 256
+REFINE_TRAFFIC_LAUNCH = "refine round over windows N/2..N at m=300, ncu dram__bytes_read+write"
 
 
 def matrix_pairs(n: int, minL: int, maxL: int) -> float:
@@ -318,7 +322,8 @@ def run_paddi(args, world, rank, local):
         achieved, ms_tc = rate(tc)
         peak = bf16 / 3.0  # three 16-bit products per FP32-accurate product
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": None, "kernel": "k_refine_umma",
+                "frac": achieved / peak, "traffic": REFINE_TRAFFIC_BYTES,
+                "traffic_launch": REFINE_TRAFFIC_LAUNCH, "kernel": "k_refine_umma",
                 "peak_source": f"bf16 dense {src} {bf16} TFLOP/s / 3 (split operands issue 3 MMAs)",
                 "work": "2*m FLOP per (candidate, window) pair evaluated",
                 "kernel_ms_per_step": ms_tc, "attempts": len(tc)}

@@ -213,7 +213,8 @@ paddi_status paddi_do_pd3(paddi_ctx *ctx, const float *d_T, size_t n, uint32_t m
  * W1[64][12] b1[64] W2[64][64] b2[64] W3[64] b3) are trained by the library's
  * own kernels; inference runs a BF16 copy.  Under PADDI_R_LEARNED the first
  * attempt of a length uses r^2 = d_{m-1} exp(y_hat) * margin, never below the
- * bound of PADDI_R_BOUND; a miss is lowered as MERLIN lowers r. */
+ * bound of PADDI_R_BOUND; after a miss r^2 drops by at least 15% (30% from the
+ * second miss on; at least MERLIN's own step), never below the bound. */
 #define PADDI_MODEL_NFEAT 12
 #define PADDI_MODEL_NPARAM 5057
 

@@ -134,7 +134,7 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
 __global__ void __launch_bounds__(P1_THREADS, 5)
 k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const float *__restrict__ mu,
          uint8_t *alive, int32_t N, int32_t m, int32_t R, int32_t max_chunks, float thr,
-         const int32_t *__restrict__ flat_count, int32_t *task_counter)
+         const int32_t *__restrict__ flat_count, int32_t *task_counter, int32_t *walked)
 {
     const bool flats = *flat_count > 0;
     extern __shared__ __align__(16) unsigned char p1_smem[];
@@ -250,6 +250,7 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
         }
         __syncthreads();
         // ---- walk the R rows
+        if (t == 0) atomicAdd(walked, 1);
         const int lim = N - cbase; // column q is a window iff q < lim
         const bool bound = (rows < R) || (R + P1_D > lim);
         if (flats) {
@@ -287,7 +288,7 @@ size_t paddi_phase1_smem(int R, int m)
 cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const float *mu,
                                     uint8_t *alive, int32_t N, int32_t m, int32_t R,
                                     int32_t max_chunks, float thr_prune,
-                                    const int32_t *flat_count, int32_t *task_counter,
+                                    const int32_t *flat_count, int32_t *task_counter, int32_t *walked,
                                     int32_t num_sms, cudaStream_t st)
 {
     if (R < 64 || R > 2048 || (R & 7) || m > P1_MAXM || max_chunks < 1)
@@ -303,6 +304,6 @@ cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const flo
     int grid = num_sms * per_sm;
     if (grid > nseg * max_chunks) grid = nseg * max_chunks;
     k_phase1<<<grid, P1_THREADS, smem, st>>>(x, wst, mu, alive, N, m, R, max_chunks, thr_prune,
-                                             flat_count, task_counter);
+                                             flat_count, task_counter, walked);
     return cudaGetLastError();
 }

@@ -232,7 +232,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
     int launches = 0;
     CK(paddi_launch_phase1_dev(x, ctx->d_wst, ctx->d_mu, ctx->d_alive, N, m, R, chunks, thr_prune,
-                               ctx->d_flatcount, &ctx->d_att->task_next, ctx->num_sms, st));
+                               ctx->d_flatcount, &ctx->d_att->task_next, &ctx->d_att->p1_walked,
+                               ctx->num_sms, st));
     ++launches;
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(paddi_launch_compact(ctx->d_alive, N, ctx->d_cand, ctx->d_rho, ctx->d_pruned,
@@ -282,7 +283,9 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     CK(cudaEventRecord(ctx->ev[2], st));
     if (ctx->trace) {
         CK(cudaEventRecord(ctx->tev[nrounds], st));
-        CK(cudaMemcpyAsync(ctx->h_trace, ctx->d_trace, sizeof(int32_t) * nrounds,
+        CK(cudaMemcpyAsync(ctx->d_trace + 7, &ctx->d_att->p1_walked, sizeof(int32_t),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ctx->h_trace, ctx->d_trace, sizeof(int32_t) * 8,
                            cudaMemcpyDeviceToHost, st));
     }
     float widen = 2.f;
@@ -334,7 +337,9 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     out->launches = launches;
     if (ctx->trace) {
         std::string line = "paddi-trace m=" + std::to_string(m) + " r2=" + std::to_string(r2) +
-                           " p1=" + std::to_string(ctx->h_res->n_p1) + " rounds:";
+                           " p1=" + std::to_string(ctx->h_res->n_p1) +
+                           " p1_tasks=" + std::to_string(ctx->h_trace[7]) + "x" + std::to_string(R) +
+                           " rounds:";
         for (int rd = 0; rd < nrounds; ++rd) {
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, ctx->tev[rd], ctx->tev[rd + 1]));

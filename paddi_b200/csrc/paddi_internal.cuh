@@ -55,7 +55,7 @@ struct PaddiAttemptDev {
     int32_t status;         // nonzero: a kernel hit an internal limit
     int32_t task_next;      // task counter of the phase-1 kernel
     int32_t list_count[2];  // lengths of the ping-pong candidate lists of the refine rounds
-    int32_t pad_;
+    int32_t p1_walked;      // phase-1 tasks that walked their rows (instrumentation)
     unsigned long long n_pairs; // pairs evaluated by the refine (instrumentation)
 };
 
@@ -84,7 +84,7 @@ cudaError_t paddi_launch_stats(const float *x, int64_t n, int32_t m, float4 *wst
 cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const float *mu,
                                     uint8_t *alive, int32_t N, int32_t m, int32_t R,
                                     int32_t max_chunks, float thr_prune,
-                                    const int32_t *flat_count, int32_t *task_counter,
+                                    const int32_t *flat_count, int32_t *task_counter, int32_t *walked,
                                     int32_t num_sms, cudaStream_t st);
 
 cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
