@@ -27,13 +27,24 @@
 // epilogue removes the shift exactly with the candidate's sum of split
 // values: rho = (D 2^-(8+e) - sum(zhat') (mu_j - shift)) inv_j.
 //
-// Pipeline per CTA (one CTA per SM, 512 TMEM columns = two 128x256 FP32
-// accumulators): while the tensor core computes tile t+1 into one
-// accumulator, the 8 warps convert the slice of tile t+2 into the free
-// shared-memory stage and run the epilogue of tile t from the other
-// accumulator (tcgen05.ld, distance, exclusion, running max, prune flags).
-// Every mbarrier wait is bounded; on timeout the kernel records status 3,
-// releases its TMEM and returns.
+// Layout of the work.  Tiles sit on a fixed grid of 2048-window blocks.  Once
+// per length, k_tile_prep converts every block's slice into its hi / lo
+// halves and its per-window epilogue data (inv_j 2^-(8+e), (mu_j - shift)
+// inv_j) in global memory (L2-resident).  The refine is then a pipeline of
+// roles inside one persistent CTA per SM, coupled only by mbarriers:
+//   * loader (one thread): bulk async copies (cp.async.bulk, no multicast)
+//     of the next tile's slice into one of two shared-memory stages, and of
+//     the current tile's window data;
+//   * MMA issuer (one thread): 3 x K'/16 tcgen05.mma of 128x256x16 per tile
+//     into one of two TMEM accumulators (all 512 columns), then commit;
+//   * epilogue (4 warps, one per TMEM lane quarter): tcgen05.ld, rho with
+//     packed f32x2 FMAs, running maxima, prune flags.
+// The candidate operand is built by all 256 threads at the start of a work
+// item.  When every candidate of the item is pruned the loader stops and
+// sends an end token through the pipeline, so all roles consume the same
+// barrier phases.  Every mbarrier wait is bounded; on timeout the kernel
+// records status 3, waits (bounded) for its own copies and MMAs, releases
+// its TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <float.h>
@@ -47,13 +58,18 @@ namespace {
 constexpr int UM_THREADS = 256;  // 8 warps
 constexpr int UM_TCMAX = 16;     // candidates per tile (M = 128); 8 for M = 64
 constexpr int UM_N = 256;        // windows at stride 8
-constexpr int UM_TW = UM_N * 8;  // windows per tile
+constexpr int UM_TW = UM_N * 8;  // windows per tile (one block of the grid)
 constexpr int UM_KMAX128 = 368;  // largest K' with M = 128 (shared-memory bound)
 constexpr int UM_KMAX64 = 736;   // largest K' with M = 64
 constexpr int ZSCALE = 8;        // zhat scaled by 2^8 before splitting
+constexpr int WD_ROW = 129;      // float4 entries per shift row of the window data (128 + pad)
+constexpr int WD_BYTES = 8 * WD_ROW * 16;
 constexpr long long UM_WAIT_CYCLES = 4000000000ll; // ~2 s at 1.9 GHz
+constexpr int EPI_WARP0 = 4;     // warps 4..7: epilogue
+constexpr int MMA_WARP = 0, LOAD_WARP = 1;
 
 __host__ __device__ constexpr int kpad_of(int m) { return ((m + 7) + 15) & ~15; }
+__host__ __device__ constexpr int slice_cnt(int kp) { return UM_TW + kp + 16; }
 
 // ------------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -80,13 +96,36 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait; false when the limit was reached.
+// Bounded wait for the completion of the phase with the given parity;
+// false when the limit was reached.
 __device__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
 {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
         if (clock64() - t0 > UM_WAIT_CYCLES) return false;
     return true;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// Bulk async copy global -> this CTA's shared memory (no multicast), completing
+// `bytes` transaction bytes on bar.  dst, src 16-byte aligned; bytes % 16 == 0.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], "
+                 "%2, [%3];" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 __device__ __forceinline__ void fence_proxy_async_smem()
@@ -146,6 +185,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// max(a, b, c) in one instruction (sm_100 three-input form)
+__device__ __forceinline__ float fmax3(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // ------------------------------------------------------------------ element types
 template <bool BF> struct E16;
 template <> struct E16<false> {
@@ -161,6 +208,71 @@ template <> struct E16<true> {
     __device__ static float back(__nv_bfloat16 v) { return __bfloat162float(v); }
 };
 
+// ------------------------------------------------------------------ tile prep
+// Block b (windows [2048 b, 2048 b + 2048)): slice x[j0 .. j0 + cnt) minus
+// x[j0], scaled by 2^e (largest magnitude just below 2^14), split into hi
+// and lo halves: bq[b * 2cnt ...] = hi, then lo.  Window data for the
+// epilogue in its read layout: shift row s = q % 8, column pair k = q / 16,
+// slot = (q / 8) % 2: wd[s * 129 + k] = {a(slot 0), a(slot 1), b(slot 0), b(slot 1)}
+// with a = inv_j 2^-(8+e) and b = (mu_j - x[j0]) inv_j (zero past N).
+constexpr int TP_THREADS = 256;
+
+template <bool BF>
+__global__ void __launch_bounds__(TP_THREADS)
+k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt,
+            const float4 *__restrict__ wst, const float *__restrict__ mu, uint16_t *__restrict__ bq,
+            float4 *__restrict__ wdq)
+{
+    using X = E16<BF>;
+    __shared__ float red[TP_THREADS / 32];
+    const int b = blockIdx.x;
+    const int64_t j0 = (int64_t)b * UM_TW;
+    const float sh = x[j0];
+    float mx = 0.f;
+    for (int p = threadIdx.x; p < cnt; p += TP_THREADS) {
+        const int64_t g = j0 + p;
+        const float v = g < nser ? x[g] - sh : 0.f;
+        mx = fmaxf(mx, fabsf(v));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    mx = 0.f;
+#pragma unroll
+    for (int w = 0; w < TP_THREADS / 32; ++w) mx = fmaxf(mx, red[w]);
+    int e = 0;
+    if (mx > 0.f) {
+        int ex;
+        frexpf(mx, &ex); // mx = f * 2^ex, f in [0.5, 1)
+        e = 14 - ex;     // mx * 2^e < 2^14
+        e = max(-100, min(100, e));
+    }
+    const float sc = ldexpf(1.f, e);
+    const float dsc = ldexpf(1.f, -(ZSCALE + e));
+    uint32_t *hi = reinterpret_cast<uint32_t *>(bq + (size_t)b * 2 * cnt);
+    uint32_t *lo = reinterpret_cast<uint32_t *>(bq + (size_t)b * 2 * cnt + cnt);
+    for (int p2 = threadIdx.x; p2 < cnt / 2; p2 += TP_THREADS) {
+        const int64_t g = j0 + 2 * p2;
+        const float u0 = (g < nser ? x[g] - sh : 0.f) * sc;
+        const float u1 = (g + 1 < nser ? x[g + 1] - sh : 0.f) * sc;
+        const typename X::T h0 = X::cvt(u0), h1 = X::cvt(u1);
+        const typename X::T l0 = X::cvt(u0 - X::back(h0)), l1 = X::cvt(u1 - X::back(h1));
+        hi[p2] = (uint32_t)reinterpret_cast<const uint16_t &>(h0) |
+                 ((uint32_t)reinterpret_cast<const uint16_t &>(h1) << 16);
+        lo[p2] = (uint32_t)reinterpret_cast<const uint16_t &>(l0) |
+                 ((uint32_t)reinterpret_cast<const uint16_t &>(l1) << 16);
+    }
+    float *wf = reinterpret_cast<float *>(wdq + (size_t)b * 8 * WD_ROW);
+    for (int q = threadIdx.x; q < UM_TW; q += TP_THREADS) {
+        const int64_t j = j0 + q; // the padded tail beyond N is zero
+        const float iv = wst[j].z, mv = mu[j];
+        const int s = q & 7, i = q >> 3, k = i >> 1, slot = i & 1;
+        wf[(s * WD_ROW + k) * 4 + slot] = iv * dsc;
+        wf[(s * WD_ROW + k) * 4 + 2 + slot] = (mv - sh) * iv;
+    }
+}
+
 // ------------------------------------------------------------------ shared memory
 struct UmLayout {
     uint32_t a_hi, a_lo, b[2][2], wd, bytes;
@@ -170,7 +282,7 @@ __host__ __device__ inline UmLayout um_layout(int MM, int kp)
 {
     UmLayout L;
     const uint32_t a_bytes = (uint32_t)MM * kp * 2;
-    const uint32_t b_bytes = ((uint32_t)(UM_TW + kp + 16) * 2 + 127) & ~127u;
+    const uint32_t b_bytes = (uint32_t)slice_cnt(kp) * 2; // multiple of 32
     L.a_hi = 0;
     L.a_lo = a_bytes;
     uint32_t o = 2 * a_bytes;
@@ -179,78 +291,35 @@ __host__ __device__ inline UmLayout um_layout(int MM, int kp)
             L.b[s][h] = o;
             o += b_bytes;
         }
-    L.wd = o; // float2 (mu, inv) per window of the current tile
-    o += UM_TW * 8;
+    L.wd = o; // window data of the current tile, directly after the stages
+    o += WD_BYTES;
     L.bytes = o;
     return L;
 }
 
 struct UmShared {
-    uint64_t mbar[2];
+    uint64_t full_b[2];    // loader -> MMA: stage holds the tile's slice (or an end token)
+    uint64_t mma_done[2];  // tcgen05.commit: the tile's MMAs are complete
+    uint64_t acc_empty[2]; // epilogue -> MMA: accumulator drained
+    uint64_t wd_full;      // loader -> epilogue: window data of the tile (or an end token)
+    uint64_t wd_empty;     // epilogue -> loader: window data consumed
+    uint64_t drain;        // final MMA drain on abort
     uint32_t tmem_base;
-    int item, abort, alive;
-    float sh[3];     // shift of the tile held by each stage (and the next one)
-    float dscale[3]; // 2^-(ZSCALE + e) of the tile
+    int item, abort, tok;
+    volatile int item_dead;
+    volatile int vb[2], vw;
     int cw[UM_TCMAX], cp[UM_TCMAX];
     float cflat[UM_TCMAX], zsum[UM_TCMAX];
     uint32_t rmax[UM_TCMAX];
-    uint8_t dead[UM_TCMAX];
+    volatile uint8_t dead[UM_TCMAX];
 };
 
-// Converts the slice of the tile starting at window j0 into stage buffers.
-// One global read per value: the values stay in registers between the
-// magnitude reduction and the split (at most CV_PER values per thread).
-constexpr int CV_PER = (UM_TW + UM_KMAX64 + 16 + UM_THREADS - 1) / UM_THREADS;
+// Completed phases of each barrier before the current work item.
+struct UmPhases {
+    uint32_t full[2], done[2], acc[2], wdf, wde;
+};
 
-template <bool BF>
-__device__ void um_convert(unsigned char *smem, const UmLayout &L, int stage, const float *x,
-                           int64_t nser, int j0, int kp, float *sh_out, float *dscale_out,
-                           float *red)
-{
-    using X = E16<BF>;
-    typename X::T *hi = reinterpret_cast<typename X::T *>(smem + L.b[stage][0]);
-    typename X::T *lo = reinterpret_cast<typename X::T *>(smem + L.b[stage][1]);
-    const int cnt = UM_TW + kp + 16;
-    const float sh = __ldg(x + j0);
-    float v[CV_PER];
-    float mx = 0.f;
-#pragma unroll
-    for (int i = 0; i < CV_PER; ++i) {
-        const int p = threadIdx.x + i * UM_THREADS;
-        const int64_t g = (int64_t)j0 + p;
-        v[i] = (p < cnt && g < nser) ? __ldg(x + g) - sh : 0.f;
-        mx = fmaxf(mx, fabsf(v[i]));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-    __syncthreads();
-    mx = 0.f;
-#pragma unroll
-    for (int w = 0; w < UM_THREADS / 32; ++w) mx = fmaxf(mx, red[w]);
-    int e = 0;
-    if (mx > 0.f) {
-        int ex;
-        frexpf(mx, &ex); // mx = f * 2^ex, f in [0.5, 1)
-        e = 14 - ex;     // mx * 2^e < 2^14
-        e = max(-100, min(100, e));
-    }
-    const float sc = ldexpf(1.f, e);
-#pragma unroll
-    for (int i = 0; i < CV_PER; ++i) {
-        const int p = threadIdx.x + i * UM_THREADS;
-        if (p < cnt) {
-            const float u = v[i] * sc;
-            const typename X::T h = X::cvt(u);
-            hi[p] = h;
-            lo[p] = X::cvt(u - X::back(h));
-        }
-    }
-    if (threadIdx.x == 0) {
-        *sh_out = sh;
-        *dscale_out = ldexpf(1.f, -(ZSCALE + e));
-    }
-}
+__device__ __forceinline__ uint32_t par(uint32_t idx) { return idx & 1u; }
 
 // MM = 128: 16 candidates, accumulator row r in TMEM lane r.
 // MM = 64:  8 candidates, accumulator row r in TMEM lane (r % 16) + 32 (r / 16)
@@ -260,6 +329,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
 k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
               const float *__restrict__ mu, const int32_t *__restrict__ cand,
               const int32_t *__restrict__ list, const int32_t *__restrict__ list_count,
+              const uint16_t *__restrict__ bq, const float4 *__restrict__ wdq,
               PaddiAttemptDev *att, uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
               int32_t jb, int32_t je, float thr, int32_t grid_ctas)
 {
@@ -269,18 +339,23 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
     constexpr int RG = MM / 8;          // 8-row core-matrix groups of A
     extern __shared__ __align__(1024) unsigned char um_smem[];
     __shared__ UmShared S;
-    __shared__ float red[UM_THREADS / 32];
     const int kp = kpad_of(m);
+    const int cnt = slice_cnt(kp);
     const UmLayout L = um_layout(MM, kp);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t nser = (int64_t)N + m - 1;
 
     const int C = *list_count;
     if (C <= 0 || je <= jb) return; // uniform: before any TMEM or barrier use
 
     if (threadIdx.x == 0) {
-        mbar_init(&S.mbar[0], 1);
-        mbar_init(&S.mbar[1], 1);
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&S.full_b[s], 1);
+            mbar_init(&S.mma_done[s], 1);
+            mbar_init(&S.acc_empty[s], 4);
+        }
+        mbar_init(&S.wd_full, 1);
+        mbar_init(&S.wd_empty, 4);
+        mbar_init(&S.drain, 1);
         S.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -295,7 +370,8 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = S.tmem_base;
-    uint32_t waits0 = 0u, waits1 = 0u; // completed waits per accumulator (parity source)
+    UmPhases ph = {{0u, 0u}, {0u, 0u}, {0u, 0u}, 0u, 0u};
+    bool mma_issued = false; // MMA thread: any MMA issued
 
     const int range = je - jb;
     const int tiles = (C + UM_TC - 1) / UM_TC;
@@ -306,11 +382,12 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
     const uint32_t idesc = idesc_f16(X::fmt, UM_M, UM_N);
     const uint32_t a_hi_s = smem_u32(um_smem + L.a_hi), a_lo_s = smem_u32(um_smem + L.a_lo);
     const int kblocks = kp / 16;
-    // epilogue geometry: lane group g (TMEM lanes 32g..32g+31), column half h
-    const int g = warp & 3, hcol = warp >> 2;
+    // epilogue geometry: lane group g (TMEM lanes 32g..32g+31)
+    const int g = warp & 3;
     const bool rowok = MM == 128 || lane < 16;
     const int row = MM == 128 ? 32 * g + lane : 16 * g + (lane & 15);
     const int cidx = row >> 3, bsh = row & 7;
+    const float4 *wd4 = reinterpret_cast<const float4 *>(um_smem + L.wd);
 
     for (;;) {
         if (threadIdx.x == 0) S.item = atomicAdd(&att->work_next, 1);
@@ -319,10 +396,6 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
         if (item >= total || S.abort) break;
         const int tile = item % tiles, split = item / tiles;
         const int j_lo = jb + split * span, j_hi = min(je, j_lo + span);
-        if (j_lo >= j_hi) { // empty split (all threads agree); keep S.item stable
-            __syncthreads();
-            continue;
-        }
         if (threadIdx.x < UM_TC) {
             const int li = tile * UM_TC + threadIdx.x;
             const bool v = li < C;
@@ -334,15 +407,19 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             S.cflat[threadIdx.x] = v ? wst[w].w : 0.f;
             S.rmax[threadIdx.x] = f2ord(-INFINITY);
         }
+        if (threadIdx.x == 0) {
+            S.item_dead = 0;
+            S.tok = -1;
+        }
         __syncthreads();
         {
             int a = threadIdx.x < UM_TC ? !S.dead[threadIdx.x] : 0;
-            if (!__syncthreads_or(a)) continue;
+            if (!__syncthreads_or(a) || j_lo >= j_hi) continue; // all threads agree
         }
         // ---- candidate operand: 16 x (hi, lo) rows of scaled zhat, then 8 shifted copies
         {
             typename X::T *zh = reinterpret_cast<typename X::T *>(um_smem + L.b[0][0]);
-            typename X::T *zl = zh + UM_TC * kp; // aliases the stage buffers (idle here)
+            typename X::T *zl = zh + UM_TC * kp; // stages + window data are idle here
             const int c = threadIdx.x >> 4, t16 = threadIdx.x & 15;
             const int w = c < UM_TC ? S.cw[c] : 0;
             const bool live = c < UM_TC && !S.dead[c];
@@ -369,7 +446,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             for (int e = threadIdx.x; e < UM_M * chunks; e += UM_THREADS) {
                 const int r = e & (UM_M - 1), kc = e / UM_M;
                 const int cc = r >> 3, b = r & 7;
-                uint32_t ph[4], pl[4];
+                uint32_t ph2[4], pl2[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int k0 = kc * 8 + 2 * q - b, k1 = k0 + 1;
@@ -383,182 +460,237 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                         h1 = zh[cc * kp + k1];
                         l1 = zl[cc * kp + k1];
                     }
-                    ph[q] = (uint32_t)reinterpret_cast<uint16_t &>(h0) |
-                            ((uint32_t)reinterpret_cast<uint16_t &>(h1) << 16);
-                    pl[q] = (uint32_t)reinterpret_cast<uint16_t &>(l0) |
-                            ((uint32_t)reinterpret_cast<uint16_t &>(l1) << 16);
+                    ph2[q] = (uint32_t)reinterpret_cast<uint16_t &>(h0) |
+                             ((uint32_t)reinterpret_cast<uint16_t &>(h1) << 16);
+                    pl2[q] = (uint32_t)reinterpret_cast<uint16_t &>(l0) |
+                             ((uint32_t)reinterpret_cast<uint16_t &>(l1) << 16);
                 }
                 const uint32_t off = (uint32_t)((kc * RG + (r >> 3)) * 128 + (r & 7) * 16);
                 *reinterpret_cast<uint4 *>(um_smem + L.a_hi + off) =
-                    make_uint4(ph[0], ph[1], ph[2], ph[3]);
+                    make_uint4(ph2[0], ph2[1], ph2[2], ph2[3]);
                 *reinterpret_cast<uint4 *>(um_smem + L.a_lo + off) =
-                    make_uint4(pl[0], pl[1], pl[2], pl[3]);
+                    make_uint4(pl2[0], pl2[1], pl2[2], pl2[3]);
             }
-            __syncthreads(); // zh/zl reads done before the stages are overwritten
+            fence_proxy_async_smem(); // A for the tensor core; stages / wd for the bulk copies
+            __syncthreads();
         }
-        // ---- tile pipeline
         const int T = (j_hi - j_lo + UM_TW - 1) / UM_TW;
-        um_convert<BF>(um_smem, L, 0, x, nser, j_lo, kp, &S.sh[0], &S.dscale[0], red);
-        fence_proxy_async_smem();
-        __syncthreads();
-        auto issue = [&](int t) { // tile t -> accumulator t&1 from stage t&1
-            const int s = t & 1;
-            const uint32_t d = tmem + (uint32_t)(s * UM_N);
-            const uint32_t bh = smem_u32(um_smem + L.b[s][0]), bl = smem_u32(um_smem + L.b[s][1]);
-            for (int kb = 0; kb < kblocks; ++kb) {
-                // K-block kb = core-matrix columns 2kb, 2kb+1; LBO = next K column of cores
-                const uint64_t ah = sdesc(a_hi_s + kb * (2 * RG * 128), RG * 128, 128);
-                const uint64_t al = sdesc(a_lo_s + kb * (2 * RG * 128), RG * 128, 128);
-                const uint64_t bhd = sdesc(bh + kb * 32, 16, 128);
-                const uint64_t bld = sdesc(bl + kb * 32, 16, 128);
-                umma_f16(d, ah, bhd, idesc, kb > 0 ? 1u : 0u);
-                umma_f16(d, ah, bld, idesc, 1u);
-                umma_f16(d, al, bhd, idesc, 1u);
+        const int blk0 = j_lo / UM_TW; // j_lo is a multiple of UM_TW
+
+        // ================================================================ roles
+        if (warp == LOAD_WARP && lane == 0) {
+            // slice of tile u into stage u&1 (after the MMAs of tile u-2 are done);
+            // an end token instead once the item is dead
+            auto load_slice = [&](int u) -> bool {
+                const int s = u & 1;
+                if (u >= 2 && !mbar_wait_bounded(&S.mma_done[s], par(ph.done[s] + ((u - 2) >> 1))))
+                    return false;
+                if (S.item_dead) {
+                    S.vb[s] = 0;
+                    S.tok = u;
+                    mbar_arrive(&S.full_b[s]);
+                    return true;
+                }
+                S.vb[s] = 1;
+                const uint16_t *src = bq + (size_t)(blk0 + u) * 2 * cnt;
+                mbar_arrive_expect_tx(&S.full_b[s], (uint32_t)(4 * cnt));
+                bulk_g2s(um_smem + L.b[s][0], src, (uint32_t)(2 * cnt), &S.full_b[s]);
+                bulk_g2s(um_smem + L.b[s][1], src + cnt, (uint32_t)(2 * cnt), &S.full_b[s]);
+                return true;
+            };
+            bool ok = load_slice(0);
+            for (int u = 0; ok && u < T; ++u) {
+                if (u + 1 < T) ok = load_slice(u + 1);
+                if (!ok) break;
+                // window data of tile u (after the epilogue is done with tile u-1)
+                if (u >= 1 && !mbar_wait_bounded(&S.wd_empty, par(ph.wde + (u - 1)))) {
+                    ok = false;
+                    break;
+                }
+                if (S.tok == u + 1) { // end token: no window data for tile u either
+                    S.vw = 0;
+                    mbar_arrive(&S.wd_full);
+                    break;
+                }
+                S.vw = 1;
+                mbar_arrive_expect_tx(&S.wd_full, (uint32_t)WD_BYTES);
+                bulk_g2s(um_smem + L.wd, wdq + (size_t)(blk0 + u) * 8 * WD_ROW, (uint32_t)WD_BYTES,
+                         &S.wd_full);
             }
-            umma_commit(&S.mbar[s]);
-        };
-        if (threadIdx.x == 0) {
-            tc_fence_after();
-            issue(0);
-        }
-        float tsh0 = S.sh[0], tds0 = S.dscale[0], tsh1 = 0.f, tds1 = 0.f;
-        if (T > 1) {
-            __syncthreads(); // S.sh[0] read before it is rewritten
-            um_convert<BF>(um_smem, L, 1, x, nser, j_lo + UM_TW, kp, &S.sh[1], &S.dscale[1], red);
-            fence_proxy_async_smem();
-        }
-        __syncthreads();
-        if (T > 1) {
-            tsh1 = S.sh[1];
-            tds1 = S.dscale[1];
-        }
-        float rmax = -INFINITY;
-        const int wc = S.cw[cidx];
-        const float zsc = S.zsum[cidx], fc = S.cflat[cidx];
-        for (int t = 0; t < T; ++t) {
-            const int s = t & 1;
-            const int j0 = j_lo + t * UM_TW;
-            if (t + 1 < T && threadIdx.x == 0) {
+            if (!ok) S.abort = 1;
+        } else if (warp == MMA_WARP && lane == 0) {
+            for (int u = 0; u < T; ++u) {
+                const int s = u & 1;
+                if (!mbar_wait_bounded(&S.full_b[s], par(ph.full[s] + (u >> 1)))) {
+                    S.abort = 1;
+                    break;
+                }
+                // the accumulator's previous tile must be drained first, also before an
+                // end token: its commit completes a phase of mma_done[s] that the
+                // epilogue may still be waiting on for tile u-2
+                if (u >= 2 &&
+                    !mbar_wait_bounded(&S.acc_empty[s], par(ph.acc[s] + ((u - 2) >> 1)))) {
+                    S.abort = 1;
+                    break;
+                }
+                if (!S.vb[s]) { // end token: pass it on (the commit also covers earlier MMAs)
+                    umma_commit(&S.mma_done[s]);
+                    break;
+                }
                 tc_fence_after();
-                issue(t + 1); // overlaps with the work below
-            }
-            // wait for tile t
-            if (threadIdx.x == 0) {
-                if (!mbar_wait_bounded(&S.mbar[s], (s ? waits1 : waits0) & 1u)) S.abort = 1;
-            }
-            __syncthreads();
-            if (s) ++waits1;
-            else ++waits0;
-            if (S.abort) break;
-            tc_fence_after();
-            const float sh = s ? tsh1 : tsh0, dsc = s ? tds1 : tds0;
-            // slice of tile t+2 into the stage tile t used (its MMAs are complete)
-            if (t + 2 < T) {
-                um_convert<BF>(um_smem, L, s, x, nser, j0 + 2 * UM_TW, kp, &S.sh[2], &S.dscale[2],
-                               red);
-                fence_proxy_async_smem();
-            }
-            // per window of tile t: (inv * dscale, (mu - shift) * inv), so that
-            // rho = D * wd.x - zsum_c * wd.y (+1 for two flat windows)
-            float2 *wd = reinterpret_cast<float2 *>(um_smem + L.wd);
-            {
-                float mv[UM_TW / UM_THREADS], iv[UM_TW / UM_THREADS];
-#pragma unroll
-                for (int i = 0; i < UM_TW / UM_THREADS; ++i) {
-                    const int q = threadIdx.x + i * UM_THREADS;
-                    mv[i] = __ldg(mu + j0 + q);    // padded tail is zero
-                    iv[i] = __ldg(&wst[j0 + q].z);
+                const uint32_t d = tmem + (uint32_t)(s * UM_N);
+                const uint32_t bh = smem_u32(um_smem + L.b[s][0]), bl = smem_u32(um_smem + L.b[s][1]);
+                for (int kb = 0; kb < kblocks; ++kb) {
+                    // K-block kb = core-matrix columns 2kb, 2kb+1; LBO = next K column of cores
+                    const uint64_t ah = sdesc(a_hi_s + kb * (2 * RG * 128), RG * 128, 128);
+                    const uint64_t al = sdesc(a_lo_s + kb * (2 * RG * 128), RG * 128, 128);
+                    const uint64_t bhd = sdesc(bh + kb * 32, 16, 128);
+                    const uint64_t bld = sdesc(bl + kb * 32, 16, 128);
+                    umma_f16(d, ah, bhd, idesc, kb > 0 ? 1u : 0u);
+                    umma_f16(d, ah, bld, idesc, 1u);
+                    umma_f16(d, al, bhd, idesc, 1u);
                 }
-#pragma unroll
-                for (int i = 0; i < UM_TW / UM_THREADS; ++i)
-                    wd[threadIdx.x + i * UM_THREADS] = make_float2(iv[i] * dsc, (mv[i] - sh) * iv[i]);
+                umma_commit(&S.mma_done[s]);
+                mma_issued = true;
             }
-            __syncthreads();
-            // ---- epilogue: 128 columns per thread; a thread needs the
-            // exclusion / range mask only when its candidate's trivial-match
-            // zone or the end of the item range reaches into the tile
-            const uint32_t tb = tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(s * UM_N + 128 * hcol);
-            const bool masked = (j0 + UM_TW > j_hi) || (wc > j0 - m + 1 && wc < j0 + UM_TW + m - 1);
-            float tmax = -INFINITY;
-#pragma unroll 1
-            for (int cb = 0; cb < 4; ++cb) {
-                uint32_t r[32];
-                tmem_ld32(tb + 32 * cb, r);
-                const int qb = 8 * (128 * hcol + 32 * cb) + bsh;
-                if (!masked && fc == 0.f) {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i) {
-                        const float2 wv = wd[qb + 8 * i];
-                        tmax = fmaxf(tmax, fmaf(__uint_as_float(r[i]), wv.x, -zsc * wv.y));
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i) {
-                        const int q = qb + 8 * i, j = j0 + q;
-                        const float2 wv = wd[q];
-                        float rho = fmaf(__uint_as_float(r[i]), wv.x, -zsc * wv.y);
-                        if (fc != 0.f && wv.x == 0.f) rho += 1.f; // two flat windows
-                        const int dd = wc > j ? wc - j : j - wc;
-                        if (j < j_hi && dd >= m - 1) tmax = fmaxf(tmax, rho);
-                    }
+        } else if (warp >= EPI_WARP0) {
+            float rmax = -INFINITY;
+            const int wc = S.cw[cidx];
+            const float zsc = S.zsum[cidx], fc = S.cflat[cidx];
+            const float2 nz2 = make_float2(-zsc, -zsc);
+            // Every lane waits (acquire) and the warp then agrees through a vote, so
+            // the warp is converged and takes the same branch at every tcgen05.ld.
+            for (int u = 0; u < T; ++u) {
+                const int s = u & 1;
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&S.wd_full, par(ph.wdf + u)))) {
+                    S.abort = 1;
+                    break;
                 }
-            }
-            if (!rowok) tmax = -INFINITY;
-            rmax = fmaxf(rmax, tmax);
-            const bool hit = tmax > thr;
-            tc_fence_before();
-            const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if (lane < UM_TC / 4 && ((bal >> (8 * lane)) & 0xFFu)) {
-                const int ci = (UM_TC / 4) * g + lane;
-                if (!S.dead[ci]) {
-                    S.dead[ci] = 1;
-                    pruned[S.cp[ci]] = 1;
+                const int vw = __shfl_sync(0xffffffffu, S.vw, 0);
+                if (!__all_sync(0xffffffffu,
+                                mbar_wait_bounded(&S.mma_done[s], par(ph.done[s] + (u >> 1))))) {
+                    S.abort = 1;
+                    break;
                 }
-            }
-            if (threadIdx.x == 0)
-                atomicAdd(&att->n_pairs, (unsigned long long)UM_TC * UM_TW);
-            __syncthreads();
-            if (t + 2 < T) { // stage parameters of tile t+2
-                if (s) {
-                    tsh1 = S.sh[2];
-                    tds1 = S.dscale[2];
-                } else {
-                    tsh0 = S.sh[2];
-                    tds0 = S.dscale[2];
-                }
-            }
-            // early abandoning: stop once every candidate of the tile is pruned
-            int alive_c = 0;
-            if (threadIdx.x < UM_TC && !S.dead[threadIdx.x]) {
-                if (__ldcg(pruned + S.cp[threadIdx.x])) S.dead[threadIdx.x] = 1;
-                else alive_c = 1;
-            }
-            if (!__syncthreads_or(alive_c)) {
-                if (t + 1 < T) { // drain the MMAs of tile t+1 before leaving the item
-                    const int s1 = (t + 1) & 1;
-                    if (threadIdx.x == 0 &&
-                        !mbar_wait_bounded(&S.mbar[s1], (s1 ? waits1 : waits0) & 1u))
+                if (!vw) { // end token; its slice twin at tile u+1 is committed too
+                    const int s1 = (u + 1) & 1;
+                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&S.mma_done[s1],
+                                                                    par(ph.done[s1] + ((u + 1) >> 1)))))
                         S.abort = 1;
-                    __syncthreads();
-                    if (s1) ++waits1;
-                    else ++waits0;
+                    break;
                 }
-                break;
-            }
-        }
-        // ---- fold the running maxima (8 shifts x 2 column halves per candidate)
-        float v = rmax;
+                tc_fence_after();
+                const int j0 = j_lo + u * UM_TW;
+                if (!__shfl_sync(0xffffffffu, S.item_dead, 0)) {
+                    const uint32_t tb = tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(s * UM_N);
+                    const bool masked = (j0 + UM_TW > j_hi) ||
+                                        (wc > j0 - m + 1 && wc < j0 + UM_TW + m - 1) || fc != 0.f;
+                    const float4 *wrow = wd4 + bsh * WD_ROW;
+                    float tmax = -INFINITY;
+#pragma unroll 1
+                    for (int cb = 0; cb < 8; ++cb) {
+                        uint32_t r[32];
+                        tmem_ld32(tb + 32 * cb, r);
+                        if (!masked) {
 #pragma unroll
-        for (int o = 4; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (rowok && (lane & 7) == 0 && v > -INFINITY) atomicMax(&S.rmax[cidx], f2ord(v));
+                            for (int i2 = 0; i2 < 16; ++i2) {
+                                const float4 wv = wrow[16 * cb + i2];
+                                const float2 dd = make_float2(__uint_as_float(r[2 * i2]),
+                                                              __uint_as_float(r[2 * i2 + 1]));
+                                const float2 rho = __ffma2_rn(
+                                    dd, make_float2(wv.x, wv.y),
+                                    __fmul2_rn(nz2, make_float2(wv.z, wv.w)));
+                                tmax = fmax3(tmax, rho.x, rho.y);
+                            }
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < 32; ++i) {
+                                const int col = 32 * cb + i;
+                                const int j = j0 + 8 * col + bsh;
+                                const float4 wv = wrow[col >> 1];
+                                const float wa = (col & 1) ? wv.y : wv.x;
+                                const float wb = (col & 1) ? wv.w : wv.z;
+                                float rho = fmaf(__uint_as_float(r[i]), wa, -zsc * wb);
+                                if (fc != 0.f && wa == 0.f) rho += 1.f; // two flat windows
+                                const int dd = wc > j ? wc - j : j - wc;
+                                if (j < j_hi && dd >= m - 1) tmax = fmaxf(tmax, rho);
+                            }
+                        }
+                    }
+                    if (!rowok) tmax = -INFINITY;
+                    rmax = fmaxf(rmax, tmax);
+                    const unsigned bal = __ballot_sync(0xffffffffu, tmax > thr);
+                    if (lane < UM_TC / 4) {
+                        const int ci = (UM_TC / 4) * g + lane;
+                        if (!S.dead[ci]) {
+                            if ((bal >> (8 * lane)) & 0xFFu) {
+                                S.dead[ci] = 1;
+                                pruned[S.cp[ci]] = 1;
+                            } else if (__ldcg(pruned + S.cp[ci])) {
+                                S.dead[ci] = 1; // pruned by another CTA's item
+                            }
+                        }
+                    }
+                    __syncwarp();
+                    if (warp == EPI_WARP0 && lane == 0) {
+                        atomicAdd(&att->n_pairs, (unsigned long long)UM_TC * UM_TW);
+                        int alive = 0;
+                        for (int c = 0; c < UM_TC; ++c) alive |= !S.dead[c];
+                        if (!alive) S.item_dead = 1;
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&S.acc_empty[s]);
+                    mbar_arrive(&S.wd_empty);
+                }
+            }
+            // fold the running maxima (8 shifts per candidate)
+            float v = rmax;
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if (rowok && (lane & 7) == 0 && v > -INFINITY) atomicMax(&S.rmax[cidx], f2ord(v));
+        }
         __syncthreads();
+        // ---- phase bookkeeping (every thread, same numbers)
+        {
+            const int tok = S.tok;                 // slice index of the end token, or -1
+            const int nb = tok >= 0 ? tok + 1 : T; // full_b / mma_done phases
+            const int nw = tok >= 0 ? tok : T;     // wd_full phases
+            const int ne = tok >= 0 ? tok - 1 : T; // acc_empty / wd_empty arrivals (tok >= 1)
+            for (int s = 0; s < 2; ++s) {
+                const uint32_t cb = (uint32_t)((nb + 1 - s) >> 1);
+                const uint32_t ce = (uint32_t)((ne + 1 - s) >> 1);
+                ph.full[s] += cb;
+                ph.done[s] += cb;
+                ph.acc[s] += ce;
+            }
+            ph.wdf += (uint32_t)nw;
+            ph.wde += (uint32_t)ne;
+        }
         if (threadIdx.x < UM_TC && tile * UM_TC + threadIdx.x < C &&
             S.rmax[threadIdx.x] != f2ord(-INFINITY))
             atomicMax(rho_max + S.cp[threadIdx.x], S.rmax[threadIdx.x]);
         __syncthreads();
         if (S.abort) break;
     }
-    if (S.abort && threadIdx.x == 0) atomicExch(&att->status, 3);
+    if (S.abort) {
+        if (threadIdx.x == 0) {
+            atomicExch(&att->status, 3);
+            if (mma_issued) { // let the MMAs in flight finish before TMEM goes away
+                umma_commit(&S.drain);
+                mbar_wait_bounded(&S.drain, 0u);
+            }
+        }
+        // bulk copies in flight complete on their barriers: wait (bounded) for
+        // the last phase of each before the shared memory goes away
+        if (threadIdx.x == 32) {
+            for (int s = 0; s < 2; ++s)
+                if (ph.full[s]) mbar_wait_bounded(&S.full_b[s], par(ph.full[s] - 1));
+            if (ph.wdf) mbar_wait_bounded(&S.wd_full, par(ph.wdf - 1));
+        }
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -581,28 +713,52 @@ bool paddi_umma_supported(int device)
 
 int paddi_umma_max_m() { return UM_KMAX64 - 7; } // kpad_of(m) <= UM_KMAX64
 
-cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *wst,
-                                     const float *mu, const int32_t *cand, const int32_t *list,
-                                     const int32_t *list_count, PaddiAttemptDev *att,
-                                     uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
-                                     cudaStream_t st)
+int32_t paddi_tile_width() { return UM_TW; }
+
+int64_t paddi_tile_blocks(int64_t N) { return (N + UM_TW - 1) / UM_TW; }
+
+int64_t paddi_tile_block_elems_max() { return 2 * (int64_t)slice_cnt(UM_KMAX64); }
+
+int64_t paddi_tile_wd_entries() { return (int64_t)8 * WD_ROW; }
+
+cudaError_t paddi_launch_tile_prep(bool bf16, const float *x, int64_t n, int32_t m,
+                                   const float4 *wst, const float *mu, uint16_t *bq, float4 *wdq,
+                                   cudaStream_t st)
 {
     const int kp = kpad_of(m);
     if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
+    const int64_t N = n - m + 1;
+    const unsigned grid = (unsigned)paddi_tile_blocks(N);
+    if (bf16)
+        k_tile_prep<true><<<grid, TP_THREADS, 0, st>>>(x, n, slice_cnt(kp), wst, mu, bq, wdq);
+    else
+        k_tile_prep<false><<<grid, TP_THREADS, 0, st>>>(x, n, slice_cnt(kp), wst, mu, bq, wdq);
+    return cudaGetLastError();
+}
+
+cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *wst,
+                                     const float *mu, const int32_t *cand, const int32_t *list,
+                                     const int32_t *list_count, const uint16_t *bq,
+                                     const float4 *wdq, PaddiAttemptDev *att, uint32_t *rho_max,
+                                     uint8_t *pruned, int32_t N, int32_t m, int32_t jb, int32_t je,
+                                     float thr_prune, int32_t num_sms, cudaStream_t st)
+{
+    const int kp = kpad_of(m);
+    if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
+    if ((jb % UM_TW) != 0 || (je % UM_TW != 0 && je != N)) return cudaErrorInvalidValue;
     const int MM = kp <= UM_KMAX128 ? 128 : 64;
     const UmLayout L = um_layout(MM, kp);
     // request at least half the SM's shared memory so one CTA owns the 512 TMEM columns
     const size_t smem = L.bytes < 120 * 1024 ? 120 * 1024 : L.bytes;
     void (*kern)(const float *, const float4 *, const float *, const int32_t *, const int32_t *,
-                 const int32_t *, PaddiAttemptDev *, uint32_t *, uint8_t *, int32_t, int32_t,
-                 int32_t, int32_t, float, int32_t);
+                 const int32_t *, const uint16_t *, const float4 *, PaddiAttemptDev *, uint32_t *,
+                 uint8_t *, int32_t, int32_t, int32_t, int32_t, float, int32_t);
     if (MM == 128) kern = bf16 ? k_refine_umma<true, 128> : k_refine_umma<false, 128>;
     else kern = bf16 ? k_refine_umma<true, 64> : k_refine_umma<false, 64>;
     cudaError_t e = paddi_raise_smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     const int grid = num_sms;
-    kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, att, rho_max, pruned,
-                                         N, m, jb, je, thr_prune, grid);
+    kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, bq, wdq, att, rho_max,
+                                         pruned, N, m, jb, je, thr_prune, grid);
     return cudaGetLastError();
 }

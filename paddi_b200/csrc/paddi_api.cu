@@ -72,6 +72,8 @@ struct paddi_ctx {
     uint8_t *d_flat = nullptr, *d_alive = nullptr, *d_pruned = nullptr;
     int32_t *d_cand = nullptr, *d_rcslot = nullptr, *d_recheck = nullptr;
     int32_t *d_list[2] = {nullptr, nullptr};
+    uint16_t *d_bq = nullptr; // tensor-core refine: split series slices per tile block
+    float4 *d_wdq = nullptr;  // tensor-core refine: epilogue window data per tile block
     // single-window exact nn (r guidance): a one-entry candidate list
     PaddiAttemptDev *d_att1 = nullptr;
     int32_t *d_one = nullptr;               // [0] = window, [1] = 0 (recheck slot)
@@ -145,6 +147,8 @@ void free_buffers(paddi_ctx *ctx)
     dfree(ctx->d_nn64);
     dfree(ctx->d_list[0]);
     dfree(ctx->d_list[1]);
+    dfree(ctx->d_bq);
+    dfree(ctx->d_wdq);
     ctx->cap_n = 0;
     ctx->rc_cap = 0;
 }
@@ -169,6 +173,11 @@ paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
     CK(cudaMalloc(&ctx->d_rho, sizeof(uint32_t) * W));
     CK(cudaMalloc(&ctx->d_list[0], sizeof(int32_t) * W));
     CK(cudaMalloc(&ctx->d_list[1], sizeof(int32_t) * W));
+    if (ctx->umma_ok) {
+        const int64_t blocks = paddi_tile_blocks((int64_t)n);
+        CK(cudaMalloc(&ctx->d_bq, sizeof(uint16_t) * (size_t)(blocks * paddi_tile_block_elems_max())));
+        CK(cudaMalloc(&ctx->d_wdq, sizeof(float4) * (size_t)(blocks * paddi_tile_wd_entries())));
+    }
     CK(cudaMalloc(&ctx->d_recheck, sizeof(int32_t) * PADDI_MAX_RECHECK));
     CK(cudaMalloc(&ctx->d_nn64, sizeof(unsigned long long) * PADDI_MAX_RECHECK));
     ctx->rc_cap = PADDI_MAX_RECHECK;
@@ -202,12 +211,17 @@ float guard_of(const paddi_ctx *ctx, int kernel)
     return kernel == PADDI_DIST_SPLIT_BF16 ? 1e-3f : 1e-4f;
 }
 
-// Statistics of length m for the series in `x` (n values).
-paddi_status run_stats(paddi_ctx *ctx, const float *x, size_t n, int m)
+// Statistics of length m for the series in `x` (n values); with `tiles`, also
+// the tensor-core refine's tile data when that kernel serves this length.
+paddi_status run_stats(paddi_ctx *ctx, const float *x, size_t n, int m, bool tiles = true)
 {
     CK(cudaMemsetAsync(ctx->d_flatcount, 0, sizeof(int32_t), ctx->st));
     CK(paddi_launch_stats(x, (int64_t)n, m, ctx->d_wst, ctx->d_mu, ctx->d_mu64, ctx->d_inv64,
                           ctx->d_flat, ctx->d_flatcount, ctx->st));
+    const int kernel = refine_kernel_for(ctx, m);
+    if (tiles && kernel != PADDI_DIST_FP32)
+        CK(paddi_launch_tile_prep(kernel == PADDI_DIST_SPLIT_BF16, x, (int64_t)n, m, ctx->d_wst,
+                                  ctx->d_mu, ctx->d_bq, ctx->d_wdq, ctx->st));
     return PADDI_OK;
 }
 
@@ -246,13 +260,17 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     const bool umma = kernel != PADDI_DIST_FP32;
     out->kernel = kernel;
     // range edges N/32, N/8, N/4, N/2, N: the first rounds prune only a small
-    // share each, so they are merged into one (fewer launches, longer items)
+    // share each, so they are merged into one (fewer launches, longer items).
+    // The tensor-core refine's tiles sit on a fixed grid: edges are rounded
+    // down to multiples of its tile width.
     constexpr int kShifts[4] = {5, 3, 2, 1};
     const int nrounds = N >= (1 << 16) ? 5 : 1;
+    const int tw = umma ? paddi_tile_width() : 1;
     int jb = 0;
     for (int rd = 0; rd < nrounds; ++rd) {
-        int je = rd == nrounds - 1 ? N : (int)((int64_t)N >> kShifts[rd]);
+        int je = rd == nrounds - 1 ? N : (int)((int64_t)N >> kShifts[rd]) / tw * tw;
         if (je > N) je = N;
+        if (je < jb) je = jb;
         const int a = rd & 1, b = a ^ 1;
         if (ctx->trace) {
             CK(cudaEventRecord(ctx->tev[rd], st));
@@ -263,9 +281,9 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         if (umma)
             CK(paddi_launch_refine_umma(kernel == PADDI_DIST_SPLIT_BF16, x, ctx->d_wst, ctx->d_mu,
                                         ctx->d_cand, ctx->d_list[a],
-                                        &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,
-                                        ctx->d_pruned, N, m, jb, je, thr_prune, ctx->num_sms,
-                                        st));
+                                        &ctx->d_att->list_count[a], ctx->d_bq, ctx->d_wdq,
+                                        ctx->d_att, ctx->d_rho, ctx->d_pruned, N, m, jb, je,
+                                        thr_prune, ctx->num_sms, st));
         else
             CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
                                         &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,
@@ -868,7 +886,7 @@ PADDI_API paddi_status paddi_compute_statistics(paddi_ctx *ctx, const float *d_T
         CK(cudaEventRecord(ctx->ev[4], user));
         CK(cudaStreamWaitEvent(ctx->st, ctx->ev[4], 0));
     }
-    s = run_stats(ctx, d_T, n, (int)m);
+    s = run_stats(ctx, d_T, n, (int)m, /*tiles=*/false);
     if (s != PADDI_OK) return s;
     CK(paddi_launch_export_stats(ctx->d_mu64, ctx->d_inv64, (int32_t)(n - m + 1), (int)m, d_mean,
                                  d_std, ctx->st));

@@ -100,12 +100,27 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
                                      int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
                                      cudaStream_t st);
 
+// Tensor-core refine over windows [jb, je) (jb a multiple of the tile width,
+// je too or je = N).  bq / wdq: the per-length tile data of
+// paddi_launch_tile_prep.
 cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *wst,
                                      const float *mu, const int32_t *cand, const int32_t *list,
-                                     const int32_t *list_count, PaddiAttemptDev *att,
-                                     uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
-                                     cudaStream_t st);
+                                     const int32_t *list_count, const uint16_t *bq,
+                                     const float4 *wdq, PaddiAttemptDev *att, uint32_t *rho_max,
+                                     uint8_t *pruned, int32_t N, int32_t m, int32_t jb, int32_t je,
+                                     float thr_prune, int32_t num_sms, cudaStream_t st);
+
+// Per-length tile data of the tensor-core refine: for every block of
+// paddi_tile_width() windows, the split 16-bit series slice (bq, at most
+// paddi_tile_block_elems_max() elements per block) and the epilogue's window
+// data (wdq, paddi_tile_wd_entries() float4 per block).
+int32_t paddi_tile_width();
+int64_t paddi_tile_blocks(int64_t N);
+int64_t paddi_tile_block_elems_max();
+int64_t paddi_tile_wd_entries();
+cudaError_t paddi_launch_tile_prep(bool bf16, const float *x, int64_t n, int32_t m,
+                                   const float4 *wst, const float *mu, uint16_t *bq, float4 *wdq,
+                                   cudaStream_t st);
 
 cudaError_t paddi_launch_list_init(const PaddiAttemptDev *att, int32_t *list, int32_t *count,
                                    cudaStream_t st);
