@@ -11,15 +11,17 @@
 //   * a persistent grid pulls (segment, chunk) tasks chunk-major from a
 //     global counter, so every segment's nearest chunk is done before any
 //     segment continues, and segments whose rows are all pruned drop out;
-//   * a task is R rows x 1024 diagonals; each thread owns the 4 diagonals
-//     4t..4t+3 and their partners 512 further on, and walks all R rows with
-//     the centred covariance update
+//   * a task is R rows x 256 diagonals, walked by one warp; each lane owns
+//     the 4 diagonals 4t..4t+3 and their partners 128 further on, and walks
+//     all R rows with the centred covariance update
 //         cov(i+1, j+1) = cov(i, j) + df_i dg_j + df_j dg_i
 //     on (diagonal, partner) pairs with packed f32x2 FMAs; the column
-//     operands come pair-packed from shared memory ((col q, col q+512) per
+//     operands come pair-packed from shared memory ((col q, col q+128) per
 //     entry, XOR-swizzled so the stride-4 ring loads are conflict-free) and
-//     rotate through a 4-entry register ring, one entry per row step;
-//   * the starting covariances of the 1024 diagonals are m-term dot products
+//     rotate through a 4-entry register ring, one entry per row step.  Short
+//     chunks let most segments stop early: after the first 256 diagonals
+//     nearly every row of most segments is pruned;
+//   * the starting covariances of the 256 diagonals are m-term dot products
 //     of the centred first row window with the shifted series;
 //   * hits are tracked as running maxima of rho (per row step over the
 //     thread's 8 diagonals; per column over the rows that touch it), and only
@@ -37,9 +39,9 @@
 
 namespace {
 
-constexpr int P1_THREADS = 128;
+constexpr int P1_THREADS = 32;                // one warp per task
 constexpr int P1_GPT = 4;                     // diagonal pairs per thread
-constexpr int P1_H = P1_THREADS * P1_GPT;     // partner offset (512)
+constexpr int P1_H = P1_THREADS * P1_GPT;     // partner offset (128)
 constexpr int P1_D = 2 * P1_H;                // diagonals per chunk
 constexpr int P1_MAXM = 1024;
 

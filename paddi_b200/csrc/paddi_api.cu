@@ -239,7 +239,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     R = (R + 7) & ~7;
     if (R < 64) R = 64;
     if (R > 1024) R = 1024;
-    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 2;
+    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 8;
     cudaStream_t st = ctx->st;
     CK(cudaEventRecord(ctx->ev[0], st));
     CK(cudaMemsetAsync(ctx->d_alive, 1, (size_t)N, st));
@@ -662,7 +662,7 @@ PADDI_API void paddi_opts_default(paddi_opts *o)
     o->distance_kernel = PADDI_DIST_AUTO;
     o->r_policy = PADDI_R_MERLIN;
     o->segment_len = 512;
-    o->phase1_chunks = 2;
+    o->phase1_chunks = 8;
     o->iter_cap = 200;
     o->guard = 0.f;
 }
@@ -1170,7 +1170,7 @@ PADDI_API paddi_status paddi_autotune(paddi_ctx *ctx, const float *series, size_
         const uint32_t b = std::min(maxL, a + 2);
         if (probes.empty() || probes.back().first != a) probes.push_back({a, b});
     }
-    const uint32_t segs[3] = {256, 512, 1024}, chunks[3] = {1, 2, 4};
+    const uint32_t segs[3] = {256, 512, 1024}, chunks[3] = {4, 8, 16};
     const paddi_opts saved = ctx->opts;
     std::vector<std::vector<paddi_discord>> ref;
     float best = FLT_MAX;
