@@ -70,6 +70,12 @@ constexpr int MMA_WARP = 0, LOAD_WARP = 1;
 
 __host__ __device__ constexpr int kpad_of(int m) { return ((m + 7) + 15) & ~15; }
 __host__ __device__ constexpr int slice_cnt(int kp) { return UM_TW + kp + 16; }
+// scratch row stride (32-bit words) of the candidate operand build: 4 words of
+// front padding + kp/2 words, rounded up to 8 modulo 32
+__host__ __device__ constexpr int zrow_words(int kp)
+{
+    return (4 + kp / 2) + ((8 - (4 + kp / 2) % 32) + 32) % 32;
+}
 
 // ------------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -307,6 +313,7 @@ struct UmShared {
     uint32_t tmem_base;
     int item, abort, tok;
     volatile int item_dead;
+    int tile_live; // live candidates at the start of the current tile (instrumentation)
     volatile int vb[2], vw;
     int cw[UM_TCMAX], cp[UM_TCMAX];
     float cflat[UM_TCMAX], zsum[UM_TCMAX];
@@ -416,23 +423,54 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             int a = threadIdx.x < UM_TC ? !S.dead[threadIdx.x] : 0;
             if (!__syncthreads_or(a) || j_lo >= j_hi) continue; // all threads agree
         }
+        if (threadIdx.x == 32) { // read by the epilogue after the barriers below
+            int alive = 0;
+            for (int c = 0; c < UM_TC; ++c) alive += !S.dead[c];
+            S.tile_live = alive;
+        }
+        const int T = (j_hi - j_lo + UM_TW - 1) / UM_TW;
+        const int blk0 = j_lo / UM_TW; // j_lo is a multiple of UM_TW
+        // the first tile's slice streams into stage 0 while the operand is built
+        // (the build's scratch is stage 1 + the window data)
+        if (warp == LOAD_WARP && lane == 0) {
+            S.vb[0] = 1;
+            const uint16_t *src = bq + (size_t)blk0 * 2 * cnt;
+            mbar_arrive_expect_tx(&S.full_b[0], (uint32_t)(4 * cnt));
+            bulk_g2s(um_smem + L.b[0][0], src, (uint32_t)(2 * cnt), &S.full_b[0]);
+            bulk_g2s(um_smem + L.b[0][1], src + cnt, (uint32_t)(2 * cnt), &S.full_b[0]);
+        }
         // ---- candidate operand: 16 x (hi, lo) rows of scaled zhat, then 8 shifted copies
         {
-            typename X::T *zh = reinterpret_cast<typename X::T *>(um_smem + L.b[0][0]);
-            typename X::T *zl = zh + UM_TC * kp; // stages + window data are idle here
+            // scratch rows of 32-bit words: 4 zero words (8 elements) of front
+            // padding, then zhat[0..kp); stride ksw words with ksw % 32 == 8, so
+            // the four candidates a warp reads sit in disjoint bank ranges
+            const int ksw = zrow_words(kp);
+            uint32_t *zhw = reinterpret_cast<uint32_t *>(um_smem + L.b[1][0]);
+            uint32_t *zlw = zhw + UM_TC * ksw;
+            typename X::T *zh = reinterpret_cast<typename X::T *>(zhw);
+            typename X::T *zl = reinterpret_cast<typename X::T *>(zlw);
             const int c = threadIdx.x >> 4, t16 = threadIdx.x & 15;
             const int w = c < UM_TC ? S.cw[c] : 0;
             const bool live = c < UM_TC && !S.dead[c];
             const float muc = live ? mu[w] : 0.f;
             const float ivc = live ? wst[w].z * 256.f : 0.f; // 2^ZSCALE
             float zs = 0.f;
+            if (c < UM_TC)
+                for (int q = 4 + (kp >> 1) + t16; q < ksw; q += 16) { // tail words
+                    zhw[c * ksw + q] = 0u;
+                    zlw[c * ksw + q] = 0u;
+                }
+            if (c < UM_TC && t16 < 4) { // front padding
+                zhw[c * ksw + t16] = 0u;
+                zlw[c * ksw + t16] = 0u;
+            }
             for (int k = t16; k < kp; k += 16) {
                 const float v = (live && k < m) ? (x[w + k] - muc) * ivc : 0.f;
                 const typename X::T h = X::cvt(v);
                 const typename X::T l = X::cvt(v - X::back(h));
                 if (c < UM_TC) {
-                    zh[c * kp + k] = h;
-                    zl[c * kp + k] = l;
+                    zh[c * 2 * ksw + 8 + k] = h;
+                    zl[c * 2 * ksw + 8 + k] = l;
                 }
                 zs += X::back(h) + X::back(l);
             }
@@ -441,29 +479,27 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             if (t16 == 0 && c < UM_TC) S.zsum[c] = zs * (1.f / 256.f);
             __syncthreads();
             // A[(c,b), k'] = z_c[k' - b] in K-major core matrices:
-            // byte offset ((k'/8)*RG + r/8)*128 + (r%8)*16 + (k'%8)*2
+            // byte offset ((k'/8)*RG + r/8)*128 + (r%8)*16 + (k'%8)*2.
+            // Elements k'-b .. k'-b+7 start at padded element p0 = 8 + 8 kc - b:
+            // five 32-bit words from word p0/2, funnel-shifted by 16 bits when p0 is odd.
             const int chunks = kp / 8;
             for (int e = threadIdx.x; e < UM_M * chunks; e += UM_THREADS) {
                 const int r = e & (UM_M - 1), kc = e / UM_M;
                 const int cc = r >> 3, b = r & 7;
-                uint32_t ph2[4], pl2[4];
+                const int p0 = 8 + 8 * kc - b;
+                const uint32_t shf = (uint32_t)(p0 & 1) * 16u;
+                const uint32_t *rh = zhw + cc * ksw + (p0 >> 1);
+                const uint32_t *rl = zlw + cc * ksw + (p0 >> 1);
+                uint32_t wh[5], wl[5], ph2[4], pl2[4];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    wh[q] = rh[q];
+                    wl[q] = rl[q];
+                }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const int k0 = kc * 8 + 2 * q - b, k1 = k0 + 1;
-                    typename X::T h0 = X::cvt(0.f), h1 = X::cvt(0.f), l0 = X::cvt(0.f),
-                                  l1 = X::cvt(0.f);
-                    if (k0 >= 0 && k0 < kp) {
-                        h0 = zh[cc * kp + k0];
-                        l0 = zl[cc * kp + k0];
-                    }
-                    if (k1 >= 0 && k1 < kp) {
-                        h1 = zh[cc * kp + k1];
-                        l1 = zl[cc * kp + k1];
-                    }
-                    ph2[q] = (uint32_t)reinterpret_cast<uint16_t &>(h0) |
-                             ((uint32_t)reinterpret_cast<uint16_t &>(h1) << 16);
-                    pl2[q] = (uint32_t)reinterpret_cast<uint16_t &>(l0) |
-                             ((uint32_t)reinterpret_cast<uint16_t &>(l1) << 16);
+                    ph2[q] = __funnelshift_r(wh[q], wh[q + 1], shf);
+                    pl2[q] = __funnelshift_r(wl[q], wl[q + 1], shf);
                 }
                 const uint32_t off = (uint32_t)((kc * RG + (r >> 3)) * 128 + (r & 7) * 16);
                 *reinterpret_cast<uint4 *>(um_smem + L.a_hi + off) =
@@ -471,11 +507,9 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 *reinterpret_cast<uint4 *>(um_smem + L.a_lo + off) =
                     make_uint4(pl2[0], pl2[1], pl2[2], pl2[3]);
             }
-            fence_proxy_async_smem(); // A for the tensor core; stages / wd for the bulk copies
+            fence_proxy_async_smem(); // A for the tensor core; scratch for the bulk copies
             __syncthreads();
         }
-        const int T = (j_hi - j_lo + UM_TW - 1) / UM_TW;
-        const int blk0 = j_lo / UM_TW; // j_lo is a multiple of UM_TW
 
         // ================================================================ roles
         if (warp == LOAD_WARP && lane == 0) {
@@ -498,7 +532,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 bulk_g2s(um_smem + L.b[s][1], src + cnt, (uint32_t)(2 * cnt), &S.full_b[s]);
                 return true;
             };
-            bool ok = load_slice(0);
+            bool ok = true; // slice 0 was issued before the operand build
             for (int u = 0; ok && u < T; ++u) {
                 if (u + 1 < T) ok = load_slice(u + 1);
                 if (!ok) break;
@@ -635,7 +669,9 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                     if (warp == EPI_WARP0 && lane == 0) {
                         atomicAdd(&att->n_pairs, (unsigned long long)UM_TC * UM_TW);
                         int alive = 0;
-                        for (int c = 0; c < UM_TC; ++c) alive |= !S.dead[c];
+                        for (int c = 0; c < UM_TC; ++c) alive += !S.dead[c];
+                        atomicAdd(&att->n_live, (unsigned long long)S.tile_live * UM_TW);
+                        S.tile_live = alive;
                         if (!alive) S.item_dead = 1;
                     }
                 }

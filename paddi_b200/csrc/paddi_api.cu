@@ -61,6 +61,7 @@ struct paddi_ctx {
     bool trace = false;
     cudaEvent_t tev[9] = {};
     int32_t *d_trace = nullptr, *h_trace = nullptr;
+    unsigned long long *h_trace64 = nullptr;
     std::string err;
     size_t cap_n = 0; // series capacity (values)
     int32_t rc_cap = 0; // FP64 recheck capacity (windows)
@@ -303,6 +304,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         CK(cudaEventRecord(ctx->tev[nrounds], st));
         CK(cudaMemcpyAsync(ctx->d_trace + 7, &ctx->d_att->p1_walked, sizeof(int32_t),
                            cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ctx->h_trace64, &ctx->d_att->n_pairs, 2 * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(ctx->h_trace, ctx->d_trace, sizeof(int32_t) * 8,
                            cudaMemcpyDeviceToHost, st));
     }
@@ -363,7 +366,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
             CK(cudaEventElapsedTime(&ms, ctx->tev[rd], ctx->tev[rd + 1]));
             line += " " + std::to_string(ctx->h_trace[rd]) + "/" + std::to_string(ms);
         }
-        std::fprintf(stderr, "%s disc=%lld\n", line.c_str(), (long long)ctx->h_res->n_disc);
+        std::fprintf(stderr, "%s disc=%lld pairs=%llu live=%llu\n", line.c_str(),
+                     (long long)ctx->h_res->n_disc, ctx->h_trace64[0], ctx->h_trace64[1]);
     }
     CK(cudaEventElapsedTime(&out->ms_phase1, ctx->ev[0], ctx->ev[1]));
     CK(cudaEventElapsedTime(&out->ms_refine, ctx->ev[1], ctx->ev[2]));
@@ -713,6 +717,7 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
         for (auto &e : ctx->tev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
         ok = ok && cudaMalloc(&ctx->d_trace, 8 * sizeof(int32_t)) == cudaSuccess;
         ok = ok && cudaMallocHost(&ctx->h_trace, 8 * sizeof(int32_t)) == cudaSuccess;
+        ok = ok && cudaMallocHost(&ctx->h_trace64, 2 * sizeof(unsigned long long)) == cudaSuccess;
     }
     ok = ok && cudaMalloc(&ctx->d_att, sizeof(PaddiAttemptDev)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
@@ -765,6 +770,7 @@ PADDI_API paddi_status paddi_ctx_destroy(paddi_ctx *ctx)
         if (e) cudaEventDestroy(e);
     if (ctx->d_trace) cudaFree(ctx->d_trace);
     if (ctx->h_trace) cudaFreeHost(ctx->h_trace);
+    if (ctx->h_trace64) cudaFreeHost(ctx->h_trace64);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
     return PADDI_OK;

@@ -57,6 +57,7 @@ struct PaddiAttemptDev {
     int32_t list_count[2];  // lengths of the ping-pong candidate lists of the refine rounds
     int32_t p1_walked;      // phase-1 tasks that walked their rows (instrumentation)
     unsigned long long n_pairs; // pairs evaluated by the refine (instrumentation)
+    unsigned long long n_live;  // of those, pairs of candidates still unpruned at the tile's start
 };
 
 // Result of one attempt, copied to the host at the end of the attempt.
