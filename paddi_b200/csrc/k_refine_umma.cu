@@ -37,9 +37,10 @@
 //     the current tile's window data;
 //   * MMA issuer (one thread): 3 x K'/16 tcgen05.mma of 128x256x16 per tile
 //     into one of two TMEM accumulators (all 512 columns), then commit;
-//   * epilogue (4 warps, one per TMEM lane quarter): tcgen05.ld, rho with
-//     packed f32x2 FMAs, running maxima, prune flags.
-// The candidate operand is built by all 256 threads at the start of a work
+//   * epilogue (8 warps, two per TMEM lane quarter, 128 columns each):
+//     double-buffered tcgen05.ld, rho with packed f32x2 FMAs, running maxima,
+//     prune flags.
+// The candidate operand is built by all 384 threads at the start of a work
 // item.  When every candidate of the item is pruned the loader stops and
 // sends an end token through the pipeline, so all roles consume the same
 // barrier phases.  Every mbarrier wait is bounded; on timeout the kernel
@@ -55,7 +56,7 @@ using paddi::f2ord;
 
 namespace {
 
-constexpr int UM_THREADS = 256;  // 8 warps
+constexpr int UM_THREADS = 384;  // 12 warps
 constexpr int UM_TCMAX = 16;     // candidates per tile (M = 128); 8 for M = 64
 constexpr int UM_N = 256;        // windows at stride 8
 constexpr int UM_TW = UM_N * 8;  // windows per tile (one block of the grid)
@@ -65,7 +66,8 @@ constexpr int ZSCALE = 8;        // zhat scaled by 2^8 before splitting
 constexpr int WD_ROW = 129;      // float4 entries per shift row of the window data (128 + pad)
 constexpr int WD_BYTES = 8 * WD_ROW * 16;
 constexpr long long UM_WAIT_CYCLES = 4000000000ll; // ~2 s at 1.9 GHz
-constexpr int EPI_WARP0 = 4;     // warps 4..7: epilogue
+constexpr int EPI_WARP0 = 4;     // warps 4..11: epilogue (two per TMEM lane quarter)
+constexpr int EPI_WARPS = 8;
 constexpr int MMA_WARP = 0, LOAD_WARP = 1;
 
 __host__ __device__ constexpr int kpad_of(int m) { return ((m + 7) + 15) & ~15; }
@@ -175,7 +177,9 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar)
         : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+// tcgen05.ld without the wait, and a wait that is tied to the destination
+// registers (so no use of them can be scheduled before it).
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t (&r)[32])
 {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
                  "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
@@ -188,7 +192,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
                    "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
                    "=r"(r[30]), "=r"(r[31])
                  : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[32])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                   "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                   "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                   "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                   "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                   "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
 }
 
 // max(a, b, c) in one instruction (sm_100 three-input form)
@@ -358,10 +374,10 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
         for (int s = 0; s < 2; ++s) {
             mbar_init(&S.full_b[s], 1);
             mbar_init(&S.mma_done[s], 1);
-            mbar_init(&S.acc_empty[s], 4);
+            mbar_init(&S.acc_empty[s], EPI_WARPS);
         }
         mbar_init(&S.wd_full, 1);
-        mbar_init(&S.wd_empty, 4);
+        mbar_init(&S.wd_empty, EPI_WARPS);
         mbar_init(&S.drain, 1);
         S.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -390,7 +406,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
     const uint32_t a_hi_s = smem_u32(um_smem + L.a_hi), a_lo_s = smem_u32(um_smem + L.a_lo);
     const int kblocks = kp / 16;
     // epilogue geometry: lane group g (TMEM lanes 32g..32g+31)
-    const int g = warp & 3;
+    const int g = warp & 3, hcol = (warp - EPI_WARP0) >> 2; // lane quarter, column half
     const bool rowok = MM == 128 || lane < 16;
     const int row = MM == 128 ? 32 * g + lane : 16 * g + (lane & 15);
     const int cidx = row >> 3, bsh = row & 7;
@@ -616,15 +632,14 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 tc_fence_after();
                 const int j0 = j_lo + u * UM_TW;
                 if (!__shfl_sync(0xffffffffu, S.item_dead, 0)) {
-                    const uint32_t tb = tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(s * UM_N);
+                    const uint32_t tb = tmem + ((uint32_t)(32 * g) << 16) +
+                                        (uint32_t)(s * UM_N + 128 * hcol);
                     const bool masked = (j0 + UM_TW > j_hi) ||
                                         (wc > j0 - m + 1 && wc < j0 + UM_TW + m - 1) || fc != 0.f;
-                    const float4 *wrow = wd4 + bsh * WD_ROW;
-                    float tmax = -INFINITY;
-#pragma unroll 1
-                    for (int cb = 0; cb < 8; ++cb) {
-                        uint32_t r[32];
-                        tmem_ld32(tb + 32 * cb, r);
+                    const float4 *wrow = wd4 + bsh * WD_ROW + 64 * hcol;
+                    float tm[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+                    // 4 chunks of 32 columns; the load of chunk cb+1 overlaps the math of cb
+                    auto chunk = [&](const uint32_t (&r)[32], int cb) {
                         if (!masked) {
 #pragma unroll
                             for (int i2 = 0; i2 < 16; ++i2) {
@@ -634,23 +649,37 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                                 const float2 rho = __ffma2_rn(
                                     dd, make_float2(wv.x, wv.y),
                                     __fmul2_rn(nz2, make_float2(wv.z, wv.w)));
-                                tmax = fmax3(tmax, rho.x, rho.y);
+                                tm[i2 & 3] = fmax3(tm[i2 & 3], rho.x, rho.y);
                             }
                         } else {
 #pragma unroll
                             for (int i = 0; i < 32; ++i) {
-                                const int col = 32 * cb + i;
+                                const int col = 128 * hcol + 32 * cb + i;
                                 const int j = j0 + 8 * col + bsh;
-                                const float4 wv = wrow[col >> 1];
-                                const float wa = (col & 1) ? wv.y : wv.x;
-                                const float wb = (col & 1) ? wv.w : wv.z;
+                                const float4 wv = wrow[(32 * cb + i) >> 1];
+                                const float wa = (i & 1) ? wv.y : wv.x;
+                                const float wb = (i & 1) ? wv.w : wv.z;
                                 float rho = fmaf(__uint_as_float(r[i]), wa, -zsc * wb);
                                 if (fc != 0.f && wa == 0.f) rho += 1.f; // two flat windows
                                 const int dd = wc > j ? wc - j : j - wc;
-                                if (j < j_hi && dd >= m - 1) tmax = fmaxf(tmax, rho);
+                                if (j < j_hi && dd >= m - 1) tm[i & 3] = fmaxf(tm[i & 3], rho);
                             }
                         }
-                    }
+                    };
+                    uint32_t ra[32], rb[32];
+                    tmem_ld32_async(tb, ra);
+                    tmem_wait_ld(ra);
+                    tmem_ld32_async(tb + 32, rb);
+                    chunk(ra, 0);
+                    tmem_wait_ld(rb);
+                    tmem_ld32_async(tb + 64, ra);
+                    chunk(rb, 1);
+                    tmem_wait_ld(ra);
+                    tmem_ld32_async(tb + 96, rb);
+                    chunk(ra, 2);
+                    tmem_wait_ld(rb);
+                    chunk(rb, 3);
+                    float tmax = fmaxf(fmaxf(tm[0], tm[1]), fmaxf(tm[2], tm[3]));
                     if (!rowok) tmax = -INFINITY;
                     rmax = fmaxf(rmax, tmax);
                     const unsigned bal = __ballot_sync(0xffffffffu, tmax > thr);
