@@ -74,8 +74,8 @@ typedef struct paddi_opts {
     int32_t device;           /* CUDA device ordinal */
     int32_t distance_kernel;  /* paddi_distance_kernel */
     int32_t r_policy;         /* paddi_r_policy */
-    uint32_t segment_len;     /* phase-1 rows per segment (reference SEGMENT_N); 0 = 512 */
-    uint32_t phase1_chunks;   /* 256-diagonal chunks a segment scans before the refine; 0 = 8 */
+    uint32_t segment_len;     /* phase-1 rows per segment (reference SEGMENT_N); 0 = 256 */
+    uint32_t phase1_chunks;   /* 256-diagonal chunks a segment scans before the refine; 0 = 12 */
     uint32_t iter_cap;        /* attempts allowed per length; 0 = 200 */
     float guard;              /* correlation guard band of the FP32/BF16 decisions; 0 = default */
     uint32_t flags;           /* PADDI_FLAG_* */
@@ -175,7 +175,7 @@ paddi_status paddi_palmad_batched(paddi_ctx *ctx, const float *const *series,
 /*
  * Autotuner: times PALMAD on short probe ranges of this series (three lengths at
  * the start, middle and end of minL..maxL) for every combination of phase-1
- * segment length {256, 512, 1024} and phase-1 chunk depth {4, 8, 16}, checks
+ * segment length {256, 384, 512} and phase-1 chunk depth {8, 12, 16}, checks
  * that all combinations return the same discords, installs the fastest in ctx
  * and copies the chosen options to *chosen.  ms (optional, 9 entries) receives
  * the probe time of each combination in the order segment-major.  No

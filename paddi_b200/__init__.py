@@ -165,7 +165,7 @@ class Context:
     """A device context (one stream, device buffers reused across calls)."""
 
     def __init__(self, device: int = 0, distance_kernel: int = DIST_AUTO,
-                 r_policy: int = R_MERLIN, segment_len: int = 512, phase1_chunks: int = 8,
+                 r_policy: int = R_MERLIN, segment_len: int = 256, phase1_chunks: int = 12,
                  iter_cap: int = 200, guard: float = 0.0, flags: int = 0, model=None,
                  model_margin: float = 1.0):
         """model: parameters for R_LEARNED (default: the bundled trained model)."""
@@ -276,7 +276,7 @@ class Context:
         self._check(lib().paddi_autotune(self._h, x.ctypes.data, len(x), minL, maxL,
                                          C.byref(o), ms.ctypes.data))
         self.opts = o
-        grid = [(sg, ch) for sg in (256, 512, 1024) for ch in (4, 8, 16)]
+        grid = [(sg, ch) for sg in (256, 384, 512) for ch in (8, 12, 16)]
         return {"segment_len": o.segment_len, "phase1_chunks": o.phase1_chunks,
                 "probe_ms": dict(zip(grid, ms.tolist()))}
 

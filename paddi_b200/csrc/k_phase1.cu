@@ -216,24 +216,22 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
         // ---- starting covariances of diagonals d0 + c0 + k and d0 + c0 + k + H
         float2 cov[P1_GPT];
         {
-            float accA[P1_GPT], accB[P1_GPT], bA[4], bB[4];
+            // (diagonal, partner) pairs with packed f32x2 FMAs: bb[i] holds the
+            // series values of both diagonals of a ring slot
+            float2 acc[P1_GPT], bb[4];
 #pragma unroll
             for (int k = 0; k < P1_GPT; ++k) {
-                accA[k] = accB[k] = 0.f;
-                bA[k] = S.xb[xpad(c0 + k)];
-                bB[k] = S.xb[xpad(c0 + P1_H + k)];
+                acc[k] = make_float2(0.f, 0.f);
+                bb[k] = make_float2(S.xb[xpad(c0 + k)], S.xb[xpad(c0 + P1_H + k)]);
             }
             for (int q0 = 0; q0 < mpad; q0 += 4) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const float a = S.xa[q0 + u];
+                    const float2 a2 = make_float2(a, a);
 #pragma unroll
-                    for (int k = 0; k < P1_GPT; ++k) {
-                        accA[k] = fmaf(a, bA[(u + k) & 3], accA[k]);
-                        accB[k] = fmaf(a, bB[(u + k) & 3], accB[k]);
-                    }
-                    bA[u] = S.xb[xpad(c0 + q0 + u + 4)];
-                    bB[u] = S.xb[xpad(c0 + P1_H + q0 + u + 4)];
+                    for (int k = 0; k < P1_GPT; ++k) acc[k] = __ffma2_rn(a2, bb[(u + k) & 3], acc[k]);
+                    bb[u] = make_float2(S.xb[xpad(c0 + q0 + u + 4)], S.xb[xpad(c0 + P1_H + q0 + u + 4)]);
                 }
             }
 #pragma unroll
@@ -241,8 +239,8 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
                 const int ja = cbase + c0 + k, jb = ja + P1_H;
                 const float mua = ja < N ? mu[ja] : shift;
                 const float mub = jb < N ? mu[jb] : shift;
-                cov[k] = make_float2(fmaf(-(mua - shift), zsum, accA[k]),
-                                     fmaf(-(mub - shift), zsum, accB[k]));
+                cov[k] = make_float2(fmaf(-(mua - shift), zsum, acc[k].x),
+                                     fmaf(-(mub - shift), zsum, acc[k].y));
             }
         }
         __syncthreads(); // xa / xb are overwritten by the (df, dg) column pairs

@@ -236,11 +236,11 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     const float thr = (float)(1.0 - (double)r2 / (2.0 * (double)m));
     const float thr_prune = thr + guard;
     int R = (int)ctx->opts.segment_len;
-    if (R <= 0) R = 512;
+    if (R <= 0) R = 256;
     R = (R + 7) & ~7;
     if (R < 64) R = 64;
     if (R > 1024) R = 1024;
-    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 8;
+    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 12;
     cudaStream_t st = ctx->st;
     CK(cudaEventRecord(ctx->ev[0], st));
     CK(cudaMemsetAsync(ctx->d_alive, 1, (size_t)N, st));
@@ -665,8 +665,8 @@ PADDI_API void paddi_opts_default(paddi_opts *o)
     o->struct_size = sizeof(paddi_opts);
     o->distance_kernel = PADDI_DIST_AUTO;
     o->r_policy = PADDI_R_MERLIN;
-    o->segment_len = 512;
-    o->phase1_chunks = 8;
+    o->segment_len = 256;
+    o->phase1_chunks = 12;
     o->iter_cap = 200;
     o->guard = 0.f;
 }
@@ -1176,7 +1176,7 @@ PADDI_API paddi_status paddi_autotune(paddi_ctx *ctx, const float *series, size_
         const uint32_t b = std::min(maxL, a + 2);
         if (probes.empty() || probes.back().first != a) probes.push_back({a, b});
     }
-    const uint32_t segs[3] = {256, 512, 1024}, chunks[3] = {4, 8, 16};
+    const uint32_t segs[3] = {256, 384, 512}, chunks[3] = {8, 12, 16};
     const paddi_opts saved = ctx->opts;
     std::vector<std::vector<paddi_discord>> ref;
     float best = FLT_MAX;

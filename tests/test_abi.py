@@ -44,7 +44,7 @@ def test_default_options():
     o = P._Opts()
     P.lib().paddi_opts_default(C.byref(o))
     assert o.struct_size == C.sizeof(P._Opts)
-    assert (o.segment_len, o.phase1_chunks, o.iter_cap) == (512, 8, 200)
+    assert (o.segment_len, o.phase1_chunks, o.iter_cap) == (256, 12, 200)
 
 
 def test_null_arguments_are_rejected_without_a_device():

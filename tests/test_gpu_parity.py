@@ -305,7 +305,7 @@ def test_autotune_picks_a_config_and_keeps_results():
     x = _series(20000, 12, "palmad")
     with P.Context() as c:
         cfg = c.autotune(x, 48, 60)
-        assert cfg["segment_len"] in (256, 512, 1024) and cfg["phase1_chunks"] in (4, 8, 16)
+        assert cfg["segment_len"] in (256, 384, 512) and cfg["phase1_chunks"] in (8, 12, 16)
         assert all(v > 0 for v in cfg["probe_ms"].values())
         got, _ = c.palmad(x, 48, 60)
     want, _ = O.palmad(x, 48, 60)
