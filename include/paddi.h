@@ -62,7 +62,7 @@ typedef enum paddi_distance_kernel {
 /* Where PALMAD's threshold for the next length comes from. */
 typedef enum paddi_r_policy {
     PADDI_R_MERLIN = 0,   /* the reference schedule, src/main.cu:136-233 */
-    PADDI_R_LEARNED = 1,  /* the learned predictor (paddi_model_*), MERLIN as fallback */
+    PADDI_R_LEARNED = 1,  /* the bound where it is tight, else the learned predictor (paddi_model_*) */
     PADDI_R_BOUND = 2     /* first try r^2 just below the exact nn, at this length, of the
                              previous length's top-1 window (a lower bound on this
                              length's top-1 distance, so the try always succeeds);
@@ -212,9 +212,11 @@ paddi_status paddi_do_pd3(paddi_ctx *ctx, const float *d_T, size_t n, uint32_t m
  * schedule is src/main.cu:136-233).  Its parameters (PADDI_MODEL_NPARAM floats:
  * W1[64][12] b1[64] W2[64][64] b2[64] W3[64] b3) are trained by the library's
  * own kernels; inference runs a BF16 copy.  Under PADDI_R_LEARNED the first
- * attempt of a length uses r^2 = d_{m-1} exp(y_hat) * margin, never below the
- * bound of PADDI_R_BOUND; after a miss r^2 drops by at least 15% (30% from the
- * second miss on; at least MERLIN's own step), never below the bound. */
+ * attempt of a length starts just below the bound of PADDI_R_BOUND when that
+ * bound exceeds MERLIN's first r, and otherwise uses
+ * r^2 = d_{m-1} exp(y_hat) * margin, never below the bound; after a miss r^2
+ * drops by at least 15% (30% from the second miss on; at least MERLIN's own
+ * step), never below the bound. */
 #define PADDI_MODEL_NFEAT 12
 #define PADDI_MODEL_NPARAM 5057
 

@@ -200,7 +200,7 @@ k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
            float r2, float thr, float guard, float widen, int32_t top_k,
            const uint8_t *__restrict__ flat, int32_t rc_cap,
            int32_t *recheck, int32_t *rc_slot, unsigned long long *nn64_ord,
-           PaddiAttemptResult *res)
+           PaddiAttemptResult *res, int32_t known_w, unsigned long long known_ord)
 {
     __shared__ long long redl[32];
     __shared__ VI redv[32];
@@ -275,7 +275,10 @@ k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
         res->n_disc = certain_d;
     }
     const int nfill = s_nr < rc_cap ? s_nr : rc_cap;
-    for (int k = threadIdx.x; k < nfill; k += FZ_THREADS) nn64_ord[k] = d2ord(INFINITY);
+    // a window whose exact nn is already known (known_w) is filled in here and
+    // skipped by the recheck
+    for (int k = threadIdx.x; k < nfill; k += FZ_THREADS)
+        nn64_ord[k] = (known_w >= 0 && cand[recheck[k]] == known_w) ? known_ord : d2ord(INFINITY);
 }
 
 // ---------------------------------------------------------------- recheck
@@ -297,7 +300,7 @@ __global__ void __launch_bounds__(RC_THREADS)
 k_recheck(const float *__restrict__ x, const double *__restrict__ mu64,
           const double *__restrict__ inv64, const uint8_t *__restrict__ flat, int32_t N,
           int32_t m, const int32_t *__restrict__ cand, const int32_t *__restrict__ recheck,
-          PaddiAttemptDev *att, unsigned long long *nn64_ord)
+          PaddiAttemptDev *att, unsigned long long *nn64_ord, int32_t known_w)
 {
     __shared__ double a[RC_MAXM];
     __shared__ double xs[RC_SPAN + RC_MAXM + (RC_SPAN + RC_MAXM) / 16 + 16];
@@ -319,6 +322,7 @@ k_recheck(const float *__restrict__ x, const double *__restrict__ mu64,
         if (item >= total) break;
         const int r = item % nr, sp = item / nr;
         const int w = cand[recheck[r]];
+        if (w == known_w) continue; // exact value filled in by the finalize step
         const double mw = mu64[w], iw = inv64[w];
         const int fw = flat[w];
         double asum = 0.0;
@@ -547,11 +551,13 @@ cudaError_t paddi_launch_finalize(const int32_t *cand, PaddiAttemptDev *att,
                                   float r2, float thr, float guard, float widen, int32_t top_k,
                                   const uint8_t *flat, int32_t rc_cap, int32_t *recheck,
                                   int32_t *rc_slot, unsigned long long *nn64_ord,
-                                  PaddiAttemptResult *res, cudaStream_t st)
+                                  PaddiAttemptResult *res, int32_t known_w,
+                                  unsigned long long known_ord, cudaStream_t st)
 {
     if (top_k < 1 || top_k > PADDI_MAX_TOPK) return cudaErrorInvalidValue;
     k_finalize<<<1, FZ_THREADS, 0, st>>>(cand, att, rho_max, pruned, m, r2, thr, guard, widen,
-                                         top_k, flat, rc_cap, recheck, rc_slot, nn64_ord, res);
+                                         top_k, flat, rc_cap, recheck, rc_slot, nn64_ord, res,
+                                         known_w, known_ord);
     return cudaGetLastError();
 }
 
@@ -559,11 +565,11 @@ cudaError_t paddi_launch_recheck(const float *x, const double *mu64, const doubl
                                  const uint8_t *flat, int32_t N, int32_t m,
                                  const int32_t *cand, const int32_t *recheck,
                                  PaddiAttemptDev *att, unsigned long long *nn64_ord,
-                                 int32_t num_sms, cudaStream_t st)
+                                 int32_t num_sms, int32_t known_w, cudaStream_t st)
 {
     if (m > RC_MAXM) return cudaErrorInvalidValue;
     k_recheck<<<num_sms * 4, RC_THREADS, 0, st>>>(x, mu64, inv64, flat, N, m, cand, recheck, att,
-                                                 nn64_ord);
+                                                 nn64_ord, known_w);
     return cudaGetLastError();
 }
 

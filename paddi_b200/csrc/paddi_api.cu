@@ -227,8 +227,10 @@ paddi_status run_stats(paddi_ctx *ctx, const float *x, size_t n, int m, bool til
 }
 
 // One (m, r2) attempt on the statistics currently in the context.
+// known_w >= 0: window whose exact FP64 nn at this length is already known
+// (its ordered image known_ord, from window_nn64); the recheck skips it.
 paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float r2, int top_k,
-                         AttemptOut *out)
+                         AttemptOut *out, int32_t known_w = -1, unsigned long long known_ord = 0)
 {
     const int32_t N = (int32_t)(n - m + 1);
     const int kernel = refine_kernel_for(ctx, m);
@@ -313,9 +315,10 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     for (int pass = 0; pass < 6; ++pass) {
         CK(paddi_launch_finalize(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned, m, r2, thr,
                                  guard, widen, top_k, ctx->d_flat, ctx->rc_cap, ctx->d_recheck,
-                                 ctx->d_rcslot, ctx->d_nn64, ctx->d_res, st));
+                                 ctx->d_rcslot, ctx->d_nn64, ctx->d_res, known_w, known_ord, st));
         CK(paddi_launch_recheck(x, ctx->d_mu64, ctx->d_inv64, ctx->d_flat, N, m, ctx->d_cand,
-                                ctx->d_recheck, ctx->d_att, ctx->d_nn64, ctx->num_sms, st));
+                                ctx->d_recheck, ctx->d_att, ctx->d_nn64, ctx->num_sms, known_w,
+                                st));
         CK(paddi_launch_select(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned,
                                ctx->d_recheck, ctx->d_rcslot, ctx->d_nn64, m, r2, thr, guard,
                                top_k, ctx->d_flat, ctx->d_res, st));
@@ -431,7 +434,7 @@ paddi_status window_nn64(paddi_ctx *ctx, const float *x, size_t n, int m, int w,
     CK(cudaMemcpyAsync(ctx->d_att1, &a1, sizeof(a1), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ctx->d_nn1, 0xff, sizeof(unsigned long long), st)); // +inf image
     CK(paddi_launch_recheck(x, ctx->d_mu64, ctx->d_inv64, ctx->d_flat, N, m, ctx->d_one,
-                            ctx->d_one + 1, ctx->d_att1, ctx->d_nn1, ctx->num_sms, st));
+                            ctx->d_one + 1, ctx->d_att1, ctx->d_nn1, ctx->num_sms, -1, st));
     CK(cudaMemcpyAsync(ctx->h_nn1, ctx->d_nn1, sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -550,6 +553,8 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
         float r = merlin_first_r(out, j, minL, &S);
         // ---- guidance: the bound and / or the model's prediction
         float ms_guide = 0.f, lbf = 0.f, lbm = 0.f; // lbm: largest r^2 below the bound
+        int32_t known_w = -1;           // the bound's window: its exact nn is known
+        unsigned long long known_ord = 0;
         int source = 0;
         if (j >= 1 && out[j - 1].ind >= 0 && (want_lb || policy == PADDI_R_LEARNED)) {
             // the previous length's top-1 window, evaluated exactly at this length:
@@ -559,6 +564,10 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
             double lb = 0.0;
             s = window_nn64(ctx, x, n, m, w, &lb);
             if (s != PADDI_OK) return s;
+            if (std::isfinite(lb)) {
+                known_w = w;
+                known_ord = *ctx->h_nn1;
+            }
             if (std::isfinite(lb) && lb > 0.0) {
                 lbf = (float)std::fmin(lb, (double)FLT_MAX);
                 const float rb = r_below(lbf);
@@ -569,6 +578,12 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
         if (policy == PADDI_R_BOUND && lbm > 0.f && lbm > r * r) {
             // tighter than MERLIN's first r and certain to find a discord (a window
             // that was flat at m-1 may have a small nn at m: then MERLIN leads)
+            r = r_below(lbf);
+            source = 2;
+        } else if (policy == PADDI_R_LEARNED && j >= 1 && lbm > 0.f && lbm > r * r) {
+            // the bound beats MERLIN's first r: start just below it (certain to find a
+            // discord, and exact whenever the previous top window stays on top, which
+            // is the common case); the model is for the lengths where it is weak
             r = r_below(lbf);
             source = 2;
         } else if (policy == PADDI_R_LEARNED && j >= 1) {
@@ -601,7 +616,7 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
                                 std::to_string(iter_cap) + " attempts");
             const float r2 = r * r;
             AttemptOut a;
-            s = run_attempt(ctx, x, n, m, r2, 1, &a);
+            s = run_attempt(ctx, x, n, m, r2, 1, &a, known_w, known_ord);
             if (s != PADDI_OK) return s;
             float ms_stats = 0.f;
             if (first) CK(cudaEventElapsedTime(&ms_stats, ctx->ev[4], ctx->ev[5]));

@@ -135,13 +135,14 @@ cudaError_t paddi_launch_finalize(const int32_t *cand, PaddiAttemptDev *att,
                                   float r2, float thr, float guard, float widen, int32_t top_k,
                                   const uint8_t *flat, int32_t rc_cap, int32_t *recheck,
                                   int32_t *rc_slot, unsigned long long *nn64_ord,
-                                  PaddiAttemptResult *res, cudaStream_t st);
+                                  PaddiAttemptResult *res, int32_t known_w,
+                                  unsigned long long known_ord, cudaStream_t st);
 
 cudaError_t paddi_launch_recheck(const float *x, const double *mu64, const double *inv64,
                                  const uint8_t *flat, int32_t N, int32_t m,
                                  const int32_t *cand, const int32_t *recheck,
                                  PaddiAttemptDev *att, unsigned long long *nn64_ord,
-                                 int32_t num_sms, cudaStream_t st);
+                                 int32_t num_sms, int32_t known_w, cudaStream_t st);
 
 cudaError_t paddi_launch_select(const int32_t *cand, PaddiAttemptDev *att,
                                 const uint32_t *rho_max, const uint8_t *pruned,
