@@ -40,6 +40,10 @@ import numpy as np  # noqa: E402
 N_SERIES = 1 << 21
 MIN_L, MAX_L = 64, 512
 WORKLOAD = "palmad n=2^21 L=64..512 top-1 (16 planted anomalies, seed 1)"
+# the large single-GPU run: ECG-like series, CPU sample from its first 2^22 points
+LARGE_N, LARGE_MIN_L, LARGE_MAX_L = 1 << 27, 128, 384
+LARGE_WORKLOAD = ("palmad n=2^27 L=128..384 top-1 (ECG-like beats, 64 altered, seed 5)")
+LARGE_CPU_POINTS = 1 << 22
 CPU_SAMPLE_N = 1 << 14          # points per CPU sample slice
 CPU_SLICES_PER_THREAD = 2
 CPU_SAMPLE_LENGTHS = 8          # lengths 64..71
@@ -173,53 +177,83 @@ def has_flat_run(s, run: int) -> bool:
     return bool(np.any(ends - starts >= run - 1))
 
 
-def cpu_sample_slices(x, count: int):
+def cpu_sample_slices(x, count: int, minl: int = MIN_L):
     """Up to `count` consecutive 2^14-point slices of the series that hold no
     flat run of MIN_L points: the reference's FP32 z-normalisation divides by
     a zero deviation on such windows and its r-schedule then never ends."""
     out = []
     for k in range(len(x) // CPU_SAMPLE_N):
         s = x[k * CPU_SAMPLE_N:(k + 1) * CPU_SAMPLE_N]
-        if not has_flat_run(s, MIN_L):
+        if not has_flat_run(s, minl):
             out.append(s)
         if len(out) == count:
             break
     return out
 
 
-def cpu_reference(x, steps: int, warmup: int, threads: int):
+def cpu_reference(x, steps: int, warmup: int, threads: int, minl: int = MIN_L):
     from oracle import oracle as O
-    maxl = MIN_L + CPU_SAMPLE_LENGTHS - 1
-    slices = cpu_sample_slices(x, CPU_SLICES_PER_THREAD * threads)
+    maxl = minl + CPU_SAMPLE_LENGTHS - 1
+    slices = cpu_sample_slices(x, CPU_SLICES_PER_THREAD * threads, minl)
     threads = min(threads, len(slices))
-    pairs = len(slices) * matrix_pairs(CPU_SAMPLE_N, MIN_L, maxl)
+    pairs = len(slices) * matrix_pairs(CPU_SAMPLE_N, minl, maxl)
     for _ in range(warmup):
-        O.ref_palmad_many(slices[:1], MIN_L, MIN_L, threads=1)
+        O.ref_palmad_many(slices[:1], minl, minl, threads=1)
     t = time.perf_counter()
     for _ in range(steps):
-        O.ref_palmad_many(slices, MIN_L, maxl, threads=threads)
+        O.ref_palmad_many(slices, minl, maxl, threads=threads)
     el = (time.perf_counter() - t) / steps
     return {"value": pairs / el, "unit": "pairs/s", "cores": threads, "kind": "reference",
             "sample": f"{len(slices)} slices of {CPU_SAMPLE_N} points of the same series "
-                      f"(slices without a flat run), lengths {MIN_L}..{maxl}, "
+                      f"(slices without a flat run), lengths {minl}..{maxl}, "
                       f"{threads} threads taking slices as they free up",
             "s_per_sample": el}
+
+
+def workload(args):
+    """(series, name) of the selected workload; fills args.n / minL / maxL."""
+    from paddi_b200 import datagen
+    if args.workload == "large":
+        args.n = args.n or LARGE_N
+        args.minL = args.minL or LARGE_MIN_L
+        args.maxL = args.maxL or LARGE_MAX_L
+        x, _ = datagen.ecg_series(n=args.n, seed=5)
+        name = LARGE_WORKLOAD if (args.n, args.minL, args.maxL) == (
+            LARGE_N, LARGE_MIN_L, LARGE_MAX_L) else f"palmad ECG-like n={args.n} L={args.minL}..{args.maxL}"
+    else:
+        args.n = args.n or N_SERIES
+        args.minL = args.minL or MIN_L
+        args.maxL = args.maxL or MAX_L
+        x, _ = datagen.palmad_series(n=args.n, seed=1)
+        name = WORKLOAD if (args.n, args.minL, args.maxL) == (N_SERIES, MIN_L, MAX_L) else \
+            f"palmad n={args.n} L={args.minL}..{args.maxL}"
+    return x, name
+
+
+def metric_name(args):
+    if args.workload == "large":
+        return "PALMAD matrix-equivalent pairs/s (n=2^27, L=128..384, top-1)"
+    return "PALMAD matrix-equivalent pairs/s (n=2^21, L=64..512, top-1)"
+
+
+def cpu_sample_of(x, args):
+    """The part of the series the CPU sample slices come from."""
+    return x[:LARGE_CPU_POINTS] if args.workload == "large" else x
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    from paddi_b200 import datagen
-    x, _ = datagen.palmad_series(n=N_SERIES, seed=1)
+    x, name = workload(args)
     threads = min(host_threads(), 64)
-    cb = cpu_reference(x, args.steps, args.warmup, threads)
-    line = {"metric": "PALMAD matrix-equivalent pairs/s (n=2^21, L=64..512, top-1)",
+    cb = cpu_reference(cpu_sample_of(x, args), args.steps, args.warmup, threads, args.minL)
+    line = {"metric": metric_name(args),
             "value": cb["value"], "unit": "pairs/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": cb["s_per_sample"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD + " (bounded CPU sample)", "n": N_SERIES,
-                       "minL": MIN_L, "maxL": MAX_L},
+            "config": {"workload": name + " (bounded CPU sample)", "n": args.n,
+                       "minL": args.minL, "maxL": args.maxL},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "pairs/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -236,10 +270,9 @@ def run_paddi(args, world, rank, local):
     import torch
 
     import paddi_b200 as P
-    from paddi_b200 import datagen
 
     torch.cuda.set_device(local)
-    x, _ = datagen.palmad_series(n=args.n, seed=1)
+    x, name = workload(args)
     n = len(x)
     dk = {"auto": P.DIST_AUTO, "fp32": P.DIST_FP32, "bf16": P.DIST_SPLIT_BF16,
           "fp16": P.DIST_SPLIT_FP16}[args.dist]
@@ -341,15 +374,13 @@ def run_paddi(args, world, rank, local):
         roof["fp32_part"] = {"achieved": a32, "ms_per_step": ms32, "attempts": len(f32)}
     launches = sum(e["n_launches"] for lg in logs for e in lg)
 
-    line = {"metric": "PALMAD matrix-equivalent pairs/s (n=2^21, L=64..512, top-1)",
+    line = {"metric": metric_name(args),
             "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": ("f16x3->f32" if any(e["refine_kernel"] == 3 for e in last) else
                       "bf16x3->f32" if tc else "f32"), "data": "synthetic",
-            "config": {"workload": WORKLOAD if (args.n, args.minL, args.maxL) ==
-                       (N_SERIES, MIN_L, MAX_L) else
-                       f"palmad n={args.n} L={args.minL}..{args.maxL}",
+            "config": {"workload": name,
                        "n": args.n, "minL": args.minL, "maxL": args.maxL,
                        "distance": args.dist, "r_policy": args.r_policy,
                        "l2": "flushed between steps (512 MB write)",
@@ -381,7 +412,7 @@ def run_paddi(args, world, rank, local):
                               "same_discords": same}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         _progress(rank, "CPU baseline")
-        cb = cpu_reference(x, 1, 0, min(host_threads(), 64))
+        cb = cpu_reference(cpu_sample_of(x, args), 1, 0, min(host_threads(), 64), args.minL)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -398,9 +429,12 @@ def main():
     ap.add_argument("--r-policy", choices=["merlin", "learned", "bound"], default="learned")
     ap.add_argument("--no-plain-form", action="store_true",
                     help="skip timing the plain FP32 + MERLIN form beside the headline")
-    ap.add_argument("--n", type=int, default=N_SERIES)
-    ap.add_argument("--minL", type=int, default=MIN_L)
-    ap.add_argument("--maxL", type=int, default=MAX_L)
+    ap.add_argument("--workload", choices=["palmad", "large"], default="palmad",
+                    help="palmad: n=2^21, L=64..512 (the headline); large: ECG-like n=2^27, "
+                         "L=128..384, CPU sample from the first 2^22 points")
+    ap.add_argument("--n", type=int, default=0)
+    ap.add_argument("--minL", type=int, default=0)
+    ap.add_argument("--maxL", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()
