@@ -158,6 +158,26 @@ paddi_status paddi_palmad_device(paddi_ctx *ctx, const float *d_series, size_t n
                                  uint32_t log_cap, uint32_t *n_log);
 
 /*
+ * Range-discord profile of one length, handed to a paddi_palmad_profiled
+ * callback after the length's final attempt: nn[i] (N = n - m + 1 entries) is
+ * the squared nn distance of window i when it is a candidate of that attempt
+ * (nn >= r^2; FP64-exact near the threshold and the top, the refine's
+ * estimate elsewhere) and -FLT_MAX otherwise, the nnDist layout of
+ * paddi_do_pd3.  The array is valid during the call only.
+ */
+typedef void (*paddi_profile_fn)(void *user, uint32_t m, const float *nn, size_t N);
+
+/*
+ * paddi_palmad plus the range-discord profile of every length, passed to fn
+ * in order of length.  The reference's writer for these rows is
+ * write_range_discord_profile (src/IOdata.hpp:90-108: m, then the N values).
+ */
+paddi_status paddi_palmad_profiled(paddi_ctx *ctx, const float *series, size_t n, uint32_t minL,
+                                   uint32_t maxL, paddi_discord *out, paddi_attempt_log *log,
+                                   uint32_t log_cap, uint32_t *n_log, paddi_profile_fn fn,
+                                   void *user);
+
+/*
  * PALMAD over many series of uneven length (each at least 2*maxL values).
  * series[k] (host pointers) has lens[k] values; out receives count*(maxL-minL+1)
  * discords, out[k*(maxL-minL+1) + i] for series k and length minL+i; status

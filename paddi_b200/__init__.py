@@ -94,6 +94,9 @@ class Discord:
 
 
 # Every exported function of include/paddi.h with its ctypes signature.
+# per-length range-discord profile callback: (user, m, nn, N)
+PROFILE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.c_size_t)
+
 _SIGS = {
     "paddi_abi_version": ([], C.c_int32),
     "paddi_status_string": ([C.c_int], C.c_char_p),
@@ -118,6 +121,9 @@ _SIGS = {
                       C.c_void_p, C.POINTER(C.c_int64), C.c_void_p], C.c_int),
     "paddi_compute_statistics_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                           C.c_uint32, C.c_void_p], C.c_int),
+    "paddi_palmad_profiled": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint32,
+                               C.POINTER(_Discord), C.POINTER(_Log), C.c_uint32,
+                               C.POINTER(C.c_uint32), PROFILE_FN, C.c_void_p], C.c_int),
     "paddi_palmad_batched": ([C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
                               C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                               C.POINTER(_Discord), C.c_void_p, C.c_void_p], C.c_int),
@@ -267,6 +273,34 @@ class Context:
                                        log_cap, C.byref(nl)))
         return ([Discord(out[i].ind, out[i].dist) for i in range(L)],
                 [log[i].as_dict() for i in range(min(nl.value, log_cap))])
+
+    def palmad_profiled(self, series, minL: int, maxL: int, on_profile=None,
+                        log_cap: int = 100000):
+        """paddi_palmad plus the range-discord profile of every length.
+
+        on_profile(m, nn) receives a copy (numpy float32, N = n - m + 1) of the
+        length's profile; without it the profiles are returned as a list.
+        Returns (discords, log, profiles or None)."""
+        x = np.ascontiguousarray(series, dtype=np.float32)
+        L = maxL - minL + 1
+        out = (_Discord * max(L, 1))()
+        log = (_Log * log_cap)()
+        nl = C.c_uint32(0)
+        kept = []
+
+        def cb(_user, m, ptr, N):
+            arr = np.ctypeslib.as_array(ptr, shape=(N,)).copy()
+            if on_profile is not None:
+                on_profile(int(m), arr)
+            else:
+                kept.append(arr)
+
+        fn = PROFILE_FN(cb)
+        self._check(lib().paddi_palmad_profiled(self._h, x.ctypes.data, len(x), minL, maxL, out,
+                                                log, log_cap, C.byref(nl), fn, None))
+        return ([Discord(out[i].ind, out[i].dist) for i in range(L)],
+                [log[i].as_dict() for i in range(min(nl.value, log_cap))],
+                None if on_profile is not None else kept)
 
     def autotune(self, series, minL: int, maxL: int):
         """Pick phase-1 segment length and depth on probe lengths of this series."""

@@ -73,6 +73,8 @@ struct paddi_ctx {
     uint8_t *d_flat = nullptr, *d_alive = nullptr, *d_pruned = nullptr;
     int32_t *d_cand = nullptr, *d_rcslot = nullptr, *d_recheck = nullptr;
     int32_t *d_list[2] = {nullptr, nullptr};
+    int32_t *d_pc = nullptr;  // range-discord profile output (allocated on first use)
+    float *d_pn = nullptr;
     uint16_t *d_bq = nullptr; // tensor-core refine: split series slices per tile block
     float4 *d_wdq = nullptr;  // tensor-core refine: epilogue window data per tile block
     // single-window exact nn (r guidance): a one-entry candidate list
@@ -150,6 +152,8 @@ void free_buffers(paddi_ctx *ctx)
     dfree(ctx->d_list[1]);
     dfree(ctx->d_bq);
     dfree(ctx->d_wdq);
+    dfree(ctx->d_pc);
+    dfree(ctx->d_pn);
     ctx->cap_n = 0;
     ctx->rc_cap = 0;
 }
@@ -524,10 +528,30 @@ paddi_status model_predict1(paddi_ctx *ctx, const float *f, float *y)
 }
 
 // PALMAD on a series already on the device.
+// Range-discord profile of the length's final attempt into prof (host, N
+// entries): the nnDist layout of paddi_do_pd3.
+paddi_status attempt_profile(paddi_ctx *ctx, int m, int32_t N, float r2, std::vector<float> &prof)
+{
+    if (!ctx->d_pc) {
+        const size_t W = ctx->cap_n + PADDI_PAD_WIN + 64;
+        CK(cudaMalloc(&ctx->d_pc, sizeof(int32_t) * W));
+        CK(cudaMalloc(&ctx->d_pn, sizeof(float) * W));
+    }
+    CK(paddi_launch_scatter(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned, ctx->d_rcslot,
+                            ctx->d_nn64, ctx->d_flat, N, m, r2, ctx->d_pc, ctx->d_pn, ctx->st));
+    prof.resize((size_t)N);
+    CK(cudaMemcpyAsync(prof.data(), ctx->d_pn, sizeof(float) * (size_t)N, cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return PADDI_OK;
+}
+
 paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL, uint32_t maxL,
                          paddi_discord *out, paddi_attempt_log *log, uint32_t log_cap,
-                         uint32_t *n_log)
+                         uint32_t *n_log, paddi_profile_fn prof_fn = nullptr,
+                         void *prof_user = nullptr)
 {
+    std::vector<float> prof;
     const int L = (int)(maxL - minL + 1);
     const int iter_cap = ctx->opts.iter_cap ? (int)ctx->opts.iter_cap : 200;
     const int policy = ctx->opts.r_policy;
@@ -656,6 +680,11 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
             }
         }
         prev_attempts = it;
+        if (prof_fn) {
+            s = attempt_profile(ctx, m, N, r * r, prof);
+            if (s != PADDI_OK) return s;
+            prof_fn(prof_user, (uint32_t)m, prof.data(), (size_t)N);
+        }
     }
     if (n_log) *n_log = nl;
     return PADDI_OK;
@@ -833,6 +862,22 @@ PADDI_API paddi_status paddi_palmad(paddi_ctx *ctx, const float *series, size_t 
     if (s != PADDI_OK) return s;
     CK(cudaMemcpyAsync(ctx->d_x, series, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->st));
     return palmad_impl(ctx, ctx->d_x, n, minL, maxL, out, log, log_cap, n_log);
+}
+
+PADDI_API paddi_status paddi_palmad_profiled(paddi_ctx *ctx, const float *series, size_t n,
+                                             uint32_t minL, uint32_t maxL, paddi_discord *out,
+                                             paddi_attempt_log *log, uint32_t log_cap,
+                                             uint32_t *n_log, paddi_profile_fn fn, void *user)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!series || !out || !fn || !valid_lengths(n, minL, maxL))
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "invalid series, lengths, output or callback");
+    if (n_log) *n_log = 0;
+    CK(cudaSetDevice(ctx->device));
+    paddi_status s = ensure_capacity(ctx, n);
+    if (s != PADDI_OK) return s;
+    CK(cudaMemcpyAsync(ctx->d_x, series, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->st));
+    return palmad_impl(ctx, ctx->d_x, n, minL, maxL, out, log, log_cap, n_log, fn, user);
 }
 
 PADDI_API paddi_status paddi_pd3(paddi_ctx *ctx, const float *series, size_t n, uint32_t m,

@@ -3,14 +3,17 @@
 // Usage (positional arguments as in src/main.cu:28-33):
 //   paddi-main <series.txt> <n> <minL> <maxL> <discords.csv> <times.csv>
 //              [--policy merlin|bound|learned] [--dist auto|fp32|bf16|fp16]
-//              [--model params.bin] [--device D]
+//              [--model params.bin] [--device D] [--profile profile.csv]
 // The series file holds one value per line (src/IOdata.hpp:63-88); the first
 // n values are used.  Outputs follow src/IOdata.hpp:111-177: the discords file
 // gets a header "m;top-1 discord idx;top-1 discord nnDist" and one row per
 // length (squared distance), the times file the reference's 14 columns, one
 // row per (length, r) attempt; both files are opened in append mode, as the
 // reference does.  The columns for MPI exchanges and host allocation are 0
-// (one GPU, one fragment, no per-attempt allocation).
+// (one GPU, one fragment, no per-attempt allocation).  --profile appends the
+// range-discord profile of every length, one row "m;v_0;...;v_{N-1}" as
+// src/IOdata.hpp:90-108 writes it (v_i: the window's squared nn distance when
+// it is a candidate of the length's final attempt, -FLT_MAX otherwise).
 #include <cfloat>
 #include <cstdio>
 #include <cstdlib>
@@ -26,7 +29,7 @@ static int usage()
     std::fprintf(stderr,
                  "usage: paddi-main <series.txt> <n> <minL> <maxL> <discords.csv> <times.csv>\n"
                  "       [--policy merlin|bound|learned] [--dist auto|fp32|bf16|fp16]\n"
-                 "       [--model params.bin] [--device D]\n");
+                 "       [--model params.bin] [--device D] [--profile profile.csv]\n");
     return 2;
 }
 
@@ -40,7 +43,7 @@ int main(int argc, char **argv)
     paddi_opts o;
     paddi_opts_default(&o);
     o.r_policy = PADDI_R_MERLIN;
-    std::string model;
+    std::string model, profile;
     for (int a = 7; a + 1 < argc; a += 2) {
         const std::string k = argv[a], v = argv[a + 1];
         if (k == "--policy")
@@ -50,6 +53,7 @@ int main(int argc, char **argv)
                                 : v == "fp16" ? PADDI_DIST_SPLIT_FP16 : PADDI_DIST_AUTO;
         else if (k == "--model") model = v;
         else if (k == "--device") o.device = std::atoi(v.c_str());
+        else if (k == "--profile") profile = v;
         else return usage();
     }
     // series: one value per line (whitespace separated), first n values
@@ -92,8 +96,20 @@ int main(int argc, char **argv)
     std::vector<paddi_discord> top(L > 0 ? L : 1);
     std::vector<paddi_attempt_log> log(1 << 16);
     uint32_t n_log = 0;
-    s = paddi_palmad(ctx, x.data(), x.size(), (uint32_t)minL, (uint32_t)maxL, top.data(),
-                     log.data(), (uint32_t)log.size(), &n_log);
+    if (profile.empty()) {
+        s = paddi_palmad(ctx, x.data(), x.size(), (uint32_t)minL, (uint32_t)maxL, top.data(),
+                         log.data(), (uint32_t)log.size(), &n_log);
+    } else {
+        std::ofstream pf(profile, std::ios::app);
+        auto write_row = [](void *user, uint32_t m, const float *nn, size_t N) {
+            std::ofstream &f = *static_cast<std::ofstream *>(user);
+            f << m << ";";
+            for (size_t i = 0; i < N; ++i) f << nn[i] << (i + 1 < N ? ";" : "\n");
+        };
+        s = paddi_palmad_profiled(ctx, x.data(), x.size(), (uint32_t)minL, (uint32_t)maxL,
+                                  top.data(), log.data(), (uint32_t)log.size(), &n_log, write_row,
+                                  &pf);
+    }
     if (s != PADDI_OK) {
         std::fprintf(stderr, "paddi_palmad: %s: %s\n", paddi_status_string(s),
                      paddi_last_error(ctx));

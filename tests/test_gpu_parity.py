@@ -111,6 +111,46 @@ def test_palmad_matches_oracle(ctx, kind, n, minL, maxL):
         assert (a["n_cand"], a["n_disc"]) == (b["n_cand"], b["n_disc"])
 
 
+def test_range_discord_profile(ctx):
+    """paddi_palmad_profiled: same discords as paddi_palmad; per length, the
+    profile marks exactly the final attempt's candidates, holds the reported
+    top-1 distance bit for bit at its window, and agrees with the oracle's
+    FP64 nn profile within the refine's guard band elsewhere."""
+    x = _series(8192, 5, "palmad")
+    minL, maxL = 40, 46
+    d, log, profs = ctx.palmad_profiled(x, minL, maxL)
+    d2, _ = ctx.palmad(x, minL, maxL)
+    assert [(q.ind, q.dist) for q in d] == [(q.ind, q.dist) for q in d2]
+    assert len(profs) == maxL - minL + 1
+    for j, p in enumerate(profs):
+        m = minL + j
+        assert p.shape == (len(x) - m + 1,)
+        last = [e for e in log if e["m"] == m][-1]
+        sel = p > -3e38
+        assert int(sel.sum()) == last["n_cand"]
+        assert p[d[j].ind] == np.float32(d[j].dist)
+        nn, _ = O.nn_profile(x, m)
+        assert np.all(np.abs(p[sel] - nn[sel]) <= 2 * m * 2e-4)
+
+
+def test_cli_writes_range_discord_profile(tmp_path):
+    import os
+    import subprocess
+    x = _series(8192, 5, "palmad")
+    f = tmp_path / "ts.txt"
+    np.savetxt(f, x, fmt="%.7g")
+    exe = os.path.join(os.path.dirname(P.__file__), "paddi-main")
+    prof = tmp_path / "profile.csv"
+    r = subprocess.run([exe, str(f), str(len(x)), "40", "42", str(tmp_path / "d.csv"),
+                        str(tmp_path / "t.csv"), "--profile", str(prof)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    rows = prof.read_text().strip().split("\n")
+    assert [int(row.split(";")[0]) for row in rows] == [40, 41, 42]
+    for row, m in zip(rows, (40, 41, 42)):
+        assert len(row.split(";")) == 1 + len(x) - m + 1
+
+
 def test_palmad_fp32_and_auto_agree(ctx, ctx32):
     x = _series(8192, 9, "palmad")
     a, la = ctx.palmad(x, 48, 56)
