@@ -266,12 +266,12 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     ++launches;
     const bool umma = kernel != PADDI_DIST_FP32;
     out->kernel = kernel;
-    // range edges N/32, N/8, N/4, N/2, N: the first rounds prune only a small
-    // share each, so they are merged into one (fewer launches, longer items).
-    // The tensor-core refine's tiles sit on a fixed grid: edges are rounded
-    // down to multiples of its tile width.
-    constexpr int kShifts[4] = {5, 3, 2, 1};
-    const int nrounds = N >= (1 << 16) ? 5 : 1;
+    // range edges N/16, N/4, N/2, N: the first rounds prune only a small share
+    // each, so they are merged (fewer launches, longer items; a sweep of 4, 5,
+    // 6 and 8 rounds picked 4).  The tensor-core refine's tiles sit on a fixed
+    // grid: edges are rounded down to multiples of its tile width.
+    constexpr int kShifts[3] = {4, 2, 1};
+    const int nrounds = N >= (1 << 16) ? 4 : 1;
     const int tw = umma ? paddi_tile_width() : 1;
     int jb = 0;
     for (int rd = 0; rd < nrounds; ++rd) {
