@@ -13,7 +13,9 @@ discords, only the number of attempts.
 
 Recipe (GPU):
     python -m paddi_b200.learned_r train --series 64 --n 131072 --minL 64 --maxL 512
-writes paddi_b200/models/r_mlp.npz; ``load_default`` reads it.
+writes paddi_b200/models/r_mlp.npz; ``load_default`` reads it.  Evaluation on
+held-out series (another seed), all three r policies:
+    python -m paddi_b200.learned_r evaluate --series 8 --n 1048576 --minL 64 --maxL 1024 --seed 97
 """
 from __future__ import annotations
 
@@ -111,9 +113,29 @@ def compare(series_list, minL, maxL, params, margin=1.0, device=0):
     return rows
 
 
+def evaluate(series_list, minL, maxL, device=0):
+    """Attempts and seconds per series for the MERLIN, BOUND and LEARNED
+    policies (same kernels); also checks that the discords are identical."""
+    from . import R_BOUND
+    rows = []
+    for x in series_list:
+        rec, ref = {}, None
+        for name, pol in (("merlin", R_MERLIN), ("bound", R_BOUND), ("learned", R_LEARNED)):
+            with Context(device=device, r_policy=pol) as ctx:
+                ctx.palmad(x, minL, minL + 2)  # warm
+                t = time.perf_counter()
+                d, log = ctx.palmad(x, minL, maxL)
+                disc = [(q.ind, q.dist) for q in d]
+                ref = disc if ref is None else ref
+                rec[name] = {"s": time.perf_counter() - t, "attempts": len(log),
+                             "same": disc == ref}
+        rows.append(rec)
+    return rows
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
-    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("cmd", choices=["train", "evaluate"])
     ap.add_argument("--series", type=int, default=64)
     ap.add_argument("--n", type=int, default=1 << 17)
     ap.add_argument("--minL", type=int, default=64)
@@ -124,6 +146,16 @@ def main(argv=None):
     ap.add_argument("--out", default=DEFAULT_MODEL)
     a = ap.parse_args(argv)
     series = datagen.training_series(a.series, a.n, a.seed, min_len=a.minL, max_len=a.maxL)
+    if a.cmd == "evaluate":
+        rows = evaluate(series, a.minL, a.maxL)
+        L = a.maxL - a.minL + 1
+        for name in ("merlin", "bound", "learned"):
+            att = sum(r[name]["attempts"] for r in rows)
+            sec = sum(r[name]["s"] for r in rows)
+            same = all(r[name]["same"] for r in rows)
+            print(f"{name:8s} attempts/length {att / (L * len(rows)):.3f}  seconds {sec:.2f}  "
+                  f"same discords {same}")
+        return
     t = time.perf_counter()
     X, Y, runs = collect(series, a.minL, a.maxL)
     t_collect = time.perf_counter() - t
