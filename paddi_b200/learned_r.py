@@ -115,7 +115,9 @@ def compare(series_list, minL, maxL, params, margin=1.0, device=0):
 
 def evaluate(series_list, minL, maxL, device=0):
     """Attempts and seconds per series for the MERLIN, BOUND and LEARNED
-    policies (same kernels); also checks that the discords are identical."""
+    policies (same kernels); checks that the discords are identical.  A
+    policy that reaches the attempt cap on a series (plain MERLIN can: its
+    decrement S of src/main.cu:230 may vanish) is recorded as None."""
     from . import R_BOUND
     rows = []
     for x in series_list:
@@ -124,7 +126,13 @@ def evaluate(series_list, minL, maxL, device=0):
             with Context(device=device, r_policy=pol) as ctx:
                 ctx.palmad(x, minL, minL + 2)  # warm
                 t = time.perf_counter()
-                d, log = ctx.palmad(x, minL, maxL)
+                try:
+                    d, log = ctx.palmad(x, minL, maxL)
+                except PaddiError as e:
+                    if e.status != PADDI_ERR_ITER_CAP:
+                        raise
+                    rec[name] = None
+                    continue
                 disc = [(q.ind, q.dist) for q in d]
                 ref = disc if ref is None else ref
                 rec[name] = {"s": time.perf_counter() - t, "attempts": len(log),
@@ -149,12 +157,16 @@ def main(argv=None):
     if a.cmd == "evaluate":
         rows = evaluate(series, a.minL, a.maxL)
         L = a.maxL - a.minL + 1
+        ok = [r for r in rows if all(r[p] is not None for p in r)]
+        print(f"series {len(rows)}; plain MERLIN reached the attempt cap on "
+              f"{sum(1 for r in rows if r['merlin'] is None)}; totals over the other {len(ok)}")
         for name in ("merlin", "bound", "learned"):
-            att = sum(r[name]["attempts"] for r in rows)
-            sec = sum(r[name]["s"] for r in rows)
-            same = all(r[name]["same"] for r in rows)
-            print(f"{name:8s} attempts/length {att / (L * len(rows)):.3f}  seconds {sec:.2f}  "
-                  f"same discords {same}")
+            att = sum(r[name]["attempts"] for r in ok)
+            sec = sum(r[name]["s"] for r in ok)
+            same = all(r[name]["same"] for r in ok)
+            capped = sum(1 for r in rows if r[name] is None)
+            print(f"{name:8s} attempts/length {att / (L * max(1, len(ok))):.3f}  seconds {sec:.2f}  "
+                  f"same discords {same}  capped {capped}")
         return
     t = time.perf_counter()
     X, Y, runs = collect(series, a.minL, a.maxL)
