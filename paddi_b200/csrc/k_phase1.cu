@@ -133,20 +133,28 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
     }
 }
 
-__global__ void __launch_bounds__(P1_THREADS, 5)
+__global__ void __launch_bounds__(P1_THREADS, 16)
 k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const float *__restrict__ mu,
          uint8_t *alive, int32_t N, int32_t m, int32_t R, int32_t max_chunks, float thr,
-         const int32_t *__restrict__ flat_count, int32_t *task_counter, int32_t *walked)
+         const int32_t *__restrict__ flat_count, int32_t *task_counter, int32_t *walked,
+         int32_t with_w, int32_t *status)
 {
-    const bool flats = *flat_count > 0;
+    // with_w = 0: the launch has no room for the flat-window column data (the
+    // host knew the length has no flat window); refuse if that is not so
+    const int fcount = *flat_count;
+    if (fcount > 0 && !with_w) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(status, 5);
+        return;
+    }
+    const bool flats = fcount > 0;
     extern __shared__ __align__(16) unsigned char p1_smem[];
     const int mpad = (m + 7) & ~7;
     const int ncp = p1_ncp(R);
     P1Smem S;
     S.roww = reinterpret_cast<float4 *>(p1_smem);
     S.colz = reinterpret_cast<float2 *>(S.roww + R);
-    S.colw = S.colz + ncp;
-    S.colxy = reinterpret_cast<float4 *>(S.colw + ncp);
+    S.colw = with_w ? S.colz + ncp : nullptr;
+    S.colxy = reinterpret_cast<float4 *>(S.colz + (with_w ? 2 : 1) * ncp);
     S.xa = reinterpret_cast<float *>(S.colxy);
     S.xb = S.xa + mpad;
     const size_t ubytes = max((size_t)16 * ncp,
@@ -190,7 +198,7 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
         for (int q = t; q < R + P1_H; q += P1_THREADS) {
             const float4 a = wst[cbase + q], b = wst[cbase + q + P1_H];
             S.colz[csw(q)] = make_float2(a.z, b.z);
-            S.colw[csw(q)] = make_float2(a.w, b.w);
+            if (with_w) S.colw[csw(q)] = make_float2(a.w, b.w);
         }
         const float mu0 = mu[i0];
         float zs = 0.f;
@@ -272,12 +280,12 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
 
 } // namespace
 
-size_t paddi_phase1_smem(int R, int m)
+size_t paddi_phase1_smem(int R, int m, bool with_w)
 {
     const int mpad = (m + 7) & ~7;
     const int ncp = p1_ncp(R);
-    size_t b = sizeof(float4) * (size_t)R;   // roww
-    b += 2 * sizeof(float2) * (size_t)ncp;   // colz, colw
+    size_t b = sizeof(float4) * (size_t)R;                  // roww
+    b += (with_w ? 2 : 1) * sizeof(float2) * (size_t)ncp;   // colz (, colw)
     const size_t ubytes = std::max((size_t)16 * ncp,
                                    (size_t)4 * (mpad + xpad(P1_D + mpad + 8) + 1));
     b += (ubytes + 15) & ~(size_t)15;        // colxy / xa + xb
@@ -289,11 +297,11 @@ cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const flo
                                     uint8_t *alive, int32_t N, int32_t m, int32_t R,
                                     int32_t max_chunks, float thr_prune,
                                     const int32_t *flat_count, int32_t *task_counter, int32_t *walked,
-                                    int32_t num_sms, cudaStream_t st)
+                                    bool with_w, int32_t *status, int32_t num_sms, cudaStream_t st)
 {
     if (R < 64 || R > 2048 || (R & 7) || m > P1_MAXM || max_chunks < 1)
         return cudaErrorInvalidValue;
-    const size_t smem = paddi_phase1_smem(R, m);
+    const size_t smem = paddi_phase1_smem(R, m, with_w);
     cudaError_t e = paddi_raise_smem_limit((const void *)k_phase1, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -304,6 +312,7 @@ cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const flo
     int grid = num_sms * per_sm;
     if (grid > nseg * max_chunks) grid = nseg * max_chunks;
     k_phase1<<<grid, P1_THREADS, smem, st>>>(x, wst, mu, alive, N, m, R, max_chunks, thr_prune,
-                                             flat_count, task_counter, walked);
+                                             flat_count, task_counter, walked, with_w ? 1 : 0,
+                                             status);
     return cudaGetLastError();
 }

@@ -86,7 +86,8 @@ cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const flo
                                     uint8_t *alive, int32_t N, int32_t m, int32_t R,
                                     int32_t max_chunks, float thr_prune,
                                     const int32_t *flat_count, int32_t *task_counter, int32_t *walked,
-                                    int32_t num_sms, cudaStream_t st);
+                                    bool with_w, int32_t *status, int32_t num_sms,
+                                    cudaStream_t st);
 
 cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
                                  uint32_t *rho_max, uint8_t *pruned, int32_t *rc_slot,
@@ -151,7 +152,9 @@ cudaError_t paddi_launch_select(const int32_t *cand, PaddiAttemptDev *att,
                                 float thr, float guard, int32_t top_k, const uint8_t *flat,
                                 PaddiAttemptResult *res, cudaStream_t st);
 
-size_t paddi_phase1_smem(int R, int m);
+// with_w: room for the flat-window column data (false only when the length is
+// known to have no flat window).
+size_t paddi_phase1_smem(int R, int m, bool with_w = true);
 
 cudaError_t paddi_launch_export_stats(const double *mu64, const double *inv64, int32_t N,
                                       int32_t m, float *mean, float *sd, cudaStream_t st);
