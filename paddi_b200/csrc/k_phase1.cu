@@ -33,6 +33,11 @@
 // window is pruned only when its FP32 correlation clears the threshold by
 // more than the rounding bound; everything else stays a candidate and is
 // settled by the refine and the FP64 recheck.
+// A flat window has inv = 0, so every pair with one gets rho = 0 here.  That
+// is exact against a non-flat window (the reference's d = 2m) and low for a
+// flat-flat pair (exactly rho = 1): such pairs prune nothing in this pass.
+// The candidate compaction drops flat windows with an admissible flat partner
+// instead, from the span of the flat windows (exact: their distance is 0).
 #include <algorithm>
 
 #include "paddi_internal.cuh"
@@ -61,7 +66,6 @@ __device__ __forceinline__ float fmax3(float a, float b, float c)
 struct P1Smem {
     float4 *roww;     // R
     float2 *colz;     // ncp: (inv_q, inv_q+H)
-    float2 *colw;     // ncp: (flat term q, q+H)
     float4 *colxy;    // ncp: (df_q, df_q+H, dg_q, dg_q+H); aliases xa / xb
     float *xa;        // mpad
     float *xb;        // xpad(D + mpad + 8)
@@ -69,20 +73,18 @@ struct P1Smem {
     uint8_t *rowflag; // R
 };
 
-template <bool FLATS, bool BOUND>
+template <bool BOUND>
 __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], int R, int rows,
                                         int lim, float thr, int t)
 {
     const int lane = threadIdx.x & 31;
     const int c0 = P1_GPT * t;
     float4 rxy[4];
-    float2 rz[4], rw[4];
+    float2 rz[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         rxy[k] = S.colxy[csw(c0 + k)];
         rz[k] = S.colz[csw(c0 + k)];
-        if (FLATS) rw[k] = S.colw[csw(c0 + k)];
-        else rw[k] = make_float2(0.f, 0.f);
     }
     float cmA[4], cmB[4];
 #pragma unroll
@@ -93,16 +95,14 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
             const int s = s0 + u;
             const float4 ri = S.roww[s];
             const float2 rix = make_float2(ri.x, ri.x), riy = make_float2(ri.y, ri.y);
-            const float2 riz = make_float2(ri.z, ri.z), riw = make_float2(ri.w, ri.w);
+            const float2 riz = make_float2(ri.z, ri.z);
             float rmax = -INFINITY;
 #pragma unroll
             for (int k = 0; k < P1_GPT; ++k) {
                 const int sl = (u + k) & 3;
                 const float2 cx = make_float2(rxy[sl].x, rxy[sl].y);
                 const float2 cy = make_float2(rxy[sl].z, rxy[sl].w);
-                float2 rho;
-                if (FLATS) rho = __ffma2_rn(__fmul2_rn(cov[k], riz), rz[sl], __fmul2_rn(riw, rw[sl]));
-                else rho = __fmul2_rn(__fmul2_rn(cov[k], riz), rz[sl]);
+                float2 rho = __fmul2_rn(__fmul2_rn(cov[k], riz), rz[sl]);
                 if (BOUND) {
                     const int q = s + c0 + k;
                     if (s >= rows || q >= lim) rho.x = -INFINITY;
@@ -122,7 +122,6 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
             const int qn = csw(s + c0 + 4);
             rxy[u] = S.colxy[qn];
             rz[u] = S.colz[qn];
-            if (FLATS) rw[u] = S.colw[qn];
         }
     }
     // columns R + c0 + e (e < 3) were touched by the last rows only
@@ -136,25 +135,15 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
 __global__ void __launch_bounds__(P1_THREADS, 16)
 k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const float *__restrict__ mu,
          uint8_t *alive, int32_t N, int32_t m, int32_t R, int32_t max_chunks, float thr,
-         const int32_t *__restrict__ flat_count, int32_t *task_counter, int32_t *walked,
-         int32_t with_w, int32_t *status)
+         int32_t *task_counter, int32_t *walked)
 {
-    // with_w = 0: the launch has no room for the flat-window column data (the
-    // host knew the length has no flat window); refuse if that is not so
-    const int fcount = *flat_count;
-    if (fcount > 0 && !with_w) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(status, 5);
-        return;
-    }
-    const bool flats = fcount > 0;
     extern __shared__ __align__(16) unsigned char p1_smem[];
     const int mpad = (m + 7) & ~7;
     const int ncp = p1_ncp(R);
     P1Smem S;
     S.roww = reinterpret_cast<float4 *>(p1_smem);
     S.colz = reinterpret_cast<float2 *>(S.roww + R);
-    S.colw = with_w ? S.colz + ncp : nullptr;
-    S.colxy = reinterpret_cast<float4 *>(S.colz + (with_w ? 2 : 1) * ncp);
+    S.colxy = reinterpret_cast<float4 *>(S.colz + ncp);
     S.xa = reinterpret_cast<float *>(S.colxy);
     S.xb = S.xa + mpad;
     const size_t ubytes = max((size_t)16 * ncp,
@@ -187,7 +176,7 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
             any = __syncthreads_or(any);
             if (!any) continue;
         }
-        // ---- stage rows, flags, the (inv, flat) column pairs and the series
+        // ---- stage rows, flags, the inv column pairs and the series
         //      slices for the start dots
         for (int s = t; s < R; s += P1_THREADS) {
             S.roww[s] = wst[i0 + s]; // zero beyond N (padded tail)
@@ -198,7 +187,6 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
         for (int q = t; q < R + P1_H; q += P1_THREADS) {
             const float4 a = wst[cbase + q], b = wst[cbase + q + P1_H];
             S.colz[csw(q)] = make_float2(a.z, b.z);
-            if (with_w) S.colw[csw(q)] = make_float2(a.w, b.w);
         }
         const float mu0 = mu[i0];
         float zs = 0.f;
@@ -261,13 +249,8 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
         if (t == 0) atomicAdd(walked, 1);
         const int lim = N - cbase; // column q is a window iff q < lim
         const bool bound = (rows < R) || (R + P1_D > lim);
-        if (flats) {
-            if (bound && thr < 0.f) p1_walk<true, true>(S, cov, R, rows, lim, thr, t);
-            else p1_walk<true, false>(S, cov, R, rows, lim, thr, t);
-        } else {
-            if (bound && thr < 0.f) p1_walk<false, true>(S, cov, R, rows, lim, thr, t);
-            else p1_walk<false, false>(S, cov, R, rows, lim, thr, t);
-        }
+        if (bound && thr < 0.f) p1_walk<true>(S, cov, R, rows, lim, thr, t);
+        else p1_walk<false>(S, cov, R, rows, lim, thr, t);
         __syncthreads();
         // ---- flush pruning marks
         for (int s = t; s < rows; s += P1_THREADS)
@@ -280,12 +263,12 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
 
 } // namespace
 
-size_t paddi_phase1_smem(int R, int m, bool with_w)
+size_t paddi_phase1_smem(int R, int m)
 {
     const int mpad = (m + 7) & ~7;
     const int ncp = p1_ncp(R);
     size_t b = sizeof(float4) * (size_t)R;                  // roww
-    b += (with_w ? 2 : 1) * sizeof(float2) * (size_t)ncp;   // colz (, colw)
+    b += sizeof(float2) * (size_t)ncp;       // colz
     const size_t ubytes = std::max((size_t)16 * ncp,
                                    (size_t)4 * (mpad + xpad(P1_D + mpad + 8) + 1));
     b += (ubytes + 15) & ~(size_t)15;        // colxy / xa + xb
@@ -296,12 +279,12 @@ size_t paddi_phase1_smem(int R, int m, bool with_w)
 cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const float *mu,
                                     uint8_t *alive, int32_t N, int32_t m, int32_t R,
                                     int32_t max_chunks, float thr_prune,
-                                    const int32_t *flat_count, int32_t *task_counter, int32_t *walked,
-                                    bool with_w, int32_t *status, int32_t num_sms, cudaStream_t st)
+                                    int32_t *task_counter, int32_t *walked, int32_t num_sms,
+                                    cudaStream_t st)
 {
     if (R < 64 || R > 2048 || (R & 7) || m > P1_MAXM || max_chunks < 1)
         return cudaErrorInvalidValue;
-    const size_t smem = paddi_phase1_smem(R, m, with_w);
+    const size_t smem = paddi_phase1_smem(R, m);
     cudaError_t e = paddi_raise_smem_limit((const void *)k_phase1, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -312,7 +295,6 @@ cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const flo
     int grid = num_sms * per_sm;
     if (grid > nseg * max_chunks) grid = nseg * max_chunks;
     k_phase1<<<grid, P1_THREADS, smem, st>>>(x, wst, mu, alive, N, m, R, max_chunks, thr_prune,
-                                             flat_count, task_counter, walked, with_w ? 1 : 0,
-                                             status);
+                                             task_counter, walked);
     return cudaGetLastError();
 }

@@ -14,6 +14,7 @@
 //       the top-k cut-off, so the selected set and the reported distances do
 //       not depend on FP32 rounding.
 #include <float.h>
+#include <limits.h>
 
 #include "paddi_internal.cuh"
 
@@ -30,15 +31,27 @@ constexpr int RC_THREADS = 256;
 constexpr int RC_MAXM = 1024;
 
 // ---------------------------------------------------------------- compact
+// With prune_flats (r^2 > 0), a flat window that has another flat window at
+// least m-1 away is no candidate: their distance is exactly 0 < r^2 under the
+// flat-window policy (src/PD3_kernels.cuh:107-108 maps 0/0 to "closer than
+// any r").  Phase 1 leaves flat-flat pairs out (rho 0 there), so this is
+// where such windows are dropped; the span {INT_MAX - lowest, highest + 1}
+// of the flat windows decides it per window.
 __global__ void __launch_bounds__(CP_THREADS)
 k_compact(const uint8_t *__restrict__ alive, int32_t N, int32_t *cand, uint32_t *rho_max,
-          uint8_t *pruned, int32_t *rc_slot, PaddiAttemptDev *att)
+          uint8_t *pruned, int32_t *rc_slot, PaddiAttemptDev *att,
+          const uint8_t *__restrict__ flat, const int32_t *__restrict__ flat_span, int32_t m,
+          int32_t prune_flats)
 {
     __shared__ int wcnt[CP_THREADS / 32];
     __shared__ int base;
     const int i = blockIdx.x * CP_THREADS + threadIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const bool a = i < N && alive[i];
+    bool a = i < N && alive[i];
+    if (a && prune_flats && flat[i]) {
+        const int lo = INT_MAX - flat_span[0], hi = flat_span[1] - 1;
+        if (i - lo >= m - 1 || hi - i >= m - 1) a = false;
+    }
     const unsigned b = __ballot_sync(0xffffffffu, a);
     if (lane == 0) wcnt[w] = __popc(b);
     __syncthreads();
@@ -539,10 +552,13 @@ cudaError_t paddi_launch_scatter(const int32_t *cand, const PaddiAttemptDev *att
 
 cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
                                  uint32_t *rho_max, uint8_t *pruned, int32_t *rc_slot,
-                                 PaddiAttemptDev *att, cudaStream_t st)
+                                 PaddiAttemptDev *att, const uint8_t *flat,
+                                 const int32_t *flat_span, int32_t m, bool prune_flats,
+                                 cudaStream_t st)
 {
     const unsigned grid = (unsigned)((N + CP_THREADS - 1) / CP_THREADS);
-    k_compact<<<grid, CP_THREADS, 0, st>>>(alive, N, cand, rho_max, pruned, rc_slot, att);
+    k_compact<<<grid, CP_THREADS, 0, st>>>(alive, N, cand, rho_max, pruned, rc_slot, att, flat,
+                                           flat_span, m, prune_flats ? 1 : 0);
     return cudaGetLastError();
 }
 

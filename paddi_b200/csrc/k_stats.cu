@@ -12,6 +12,7 @@
 //     count of equal neighbours.
 // HBM traffic per length: 4 B read + 37 B written per window.
 #include <float.h>
+#include <limits.h>
 
 #include "paddi_internal.cuh"
 
@@ -52,7 +53,8 @@ __device__ T block_exclusive_scan(T v, T *warp_tot)
 
 __global__ void __launch_bounds__(ST_THREADS)
 k_window_stats(const float *__restrict__ x, int64_t n, int32_t m, int32_t N, float4 *wst,
-               float *mu, double *mu64, double *inv64, uint8_t *flat, int32_t *flat_count)
+               float *mu, double *mu64, double *inv64, uint8_t *flat, int32_t *flat_count,
+               int32_t *flat_span)
 {
     // staged values: x[t0 .. t0 + ST_TILE + m] (one extra window for mu_{i+1})
     __shared__ double P1[ST_TILE + ST_MAXM + 2];
@@ -138,6 +140,12 @@ k_window_stats(const float *__restrict__ x, int64_t n, int32_t m, int32_t N, flo
         inv64[i] = iv;
         flat[i] = (uint8_t)fl;
         nflat += fl;
+        // lowest and highest flat window, both kept as maxima over a zeroed
+        // pair: {INT_MAX - lowest, highest + 1} (flat windows are rare)
+        if (fl && flat_span) {
+            atomicMax(flat_span, INT_MAX - (int)i);
+            atomicMax(flat_span + 1, (int)i + 1);
+        }
     }
     if (nflat) atomicAdd(flat_count, nflat);
 }
@@ -164,13 +172,13 @@ cudaError_t paddi_launch_export_stats(const double *mu64, const double *inv64, i
 
 cudaError_t paddi_launch_stats(const float *x, int64_t n, int32_t m, float4 *wst, float *mu,
                                double *mu64, double *inv64, uint8_t *flat,
-                               int32_t *flat_count, cudaStream_t st)
+                               int32_t *flat_count, cudaStream_t st, int32_t *flat_span)
 {
     if (m < 2 || m > ST_MAXM || n < 2 * (int64_t)m) return cudaErrorInvalidValue;
     const int32_t N = (int32_t)(n - m + 1);
     const int64_t total = (int64_t)N + PADDI_PAD_WIN;
     const unsigned grid = (unsigned)((total + ST_TILE - 1) / ST_TILE);
     k_window_stats<<<grid, ST_THREADS, 0, st>>>(x, n, m, N, wst, mu, mu64, inv64, flat,
-                                                flat_count);
+                                                flat_count, flat_span);
     return cudaGetLastError();
 }

@@ -59,9 +59,6 @@ struct paddi_ctx {
     // PADDI_TRACE=1 in the environment: one stderr line per attempt with the
     // live-candidate count and the time of every refine round
     bool trace = false;
-    // the current length is known (host copy synced) to have no flat window:
-    // phase 1 then launches without room for the flat-window column data
-    bool no_flats = false;
     cudaEvent_t tev[9] = {};
     int32_t *d_trace = nullptr, *h_trace = nullptr;
     unsigned long long *h_trace64 = nullptr;
@@ -223,10 +220,10 @@ float guard_of(const paddi_ctx *ctx, int kernel)
 // the tensor-core refine's tile data when that kernel serves this length.
 paddi_status run_stats(paddi_ctx *ctx, const float *x, size_t n, int m, bool tiles = true)
 {
-    ctx->no_flats = false; // until the new length's flat count is known on the host
-    CK(cudaMemsetAsync(ctx->d_flatcount, 0, sizeof(int32_t), ctx->st));
+    // d_flatcount = {flat windows, span of the flat windows (two ints)}
+    CK(cudaMemsetAsync(ctx->d_flatcount, 0, 3 * sizeof(int32_t), ctx->st));
     CK(paddi_launch_stats(x, (int64_t)n, m, ctx->d_wst, ctx->d_mu, ctx->d_mu64, ctx->d_inv64,
-                          ctx->d_flat, ctx->d_flatcount, ctx->st));
+                          ctx->d_flat, ctx->d_flatcount, ctx->st, ctx->d_flatcount + 1));
     const int kernel = refine_kernel_for(ctx, m);
     if (tiles && kernel != PADDI_DIST_FP32)
         CK(paddi_launch_tile_prep(kernel == PADDI_DIST_SPLIT_BF16, x, (int64_t)n, m, ctx->d_wst,
@@ -257,12 +254,12 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
     int launches = 0;
     CK(paddi_launch_phase1_dev(x, ctx->d_wst, ctx->d_mu, ctx->d_alive, N, m, R, chunks, thr_prune,
-                               ctx->d_flatcount, &ctx->d_att->task_next, &ctx->d_att->p1_walked,
-                               !ctx->no_flats, &ctx->d_att->status, ctx->num_sms, st));
+                               &ctx->d_att->task_next, &ctx->d_att->p1_walked, ctx->num_sms, st));
     ++launches;
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(paddi_launch_compact(ctx->d_alive, N, ctx->d_cand, ctx->d_rho, ctx->d_pruned,
-                            ctx->d_rcslot, ctx->d_att, st));
+                            ctx->d_rcslot, ctx->d_att, ctx->d_flat, ctx->d_flatcount + 1, m,
+                            r2 > 0.f, st));
     ++launches;
     // refine rounds over growing window ranges; survivors are re-compacted
     // between rounds so every tile is dense with live candidates
@@ -355,9 +352,6 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     }
     if (ctx->h_res->status == 3)
         return fail(ctx, PADDI_ERR_CUDA, "tensor-core refine: a barrier wait timed out");
-    if (ctx->h_res->status == 5)
-        return fail(ctx, PADDI_ERR_INTERNAL_LIMIT,
-                    "phase 1 launched without flat-window data on a length with flat windows");
     if (ctx->h_res->status == 1)
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT,
                     "more windows than the FP64 recheck capacity fall inside the guard band (m=" +
@@ -606,7 +600,6 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
             }
         }
         const float flat_frac = (float)*ctx->h_flatcount / (float)N; // synced above when guided
-        if (lbf > 0.f || known_w >= 0) ctx->no_flats = *ctx->h_flatcount == 0; // synced
         if (policy == PADDI_R_BOUND && lbm > 0.f && lbm > r * r) {
             // tighter than MERLIN's first r and certain to find a discord (a window
             // that was flat at m-1 may have a small nn at m: then MERLIN leads)
@@ -773,7 +766,7 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
     }
     ok = ok && cudaMalloc(&ctx->d_att, sizeof(PaddiAttemptDev)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
-    ok = ok && cudaMalloc(&ctx->d_flatcount, sizeof(int32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_flatcount, 3 * sizeof(int32_t)) == cudaSuccess;
     ok = ok && cudaMallocHost(&ctx->h_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_att1, sizeof(PaddiAttemptDev)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_one, 2 * sizeof(int32_t)) == cudaSuccess;

@@ -80,18 +80,24 @@ struct PaddiAttemptResult {
 // All launch wrappers enqueue on `st` and return cudaGetLastError().
 cudaError_t paddi_launch_stats(const float *x, int64_t n, int32_t m, float4 *wst, float *mu,
                                double *mu64, double *inv64, uint8_t *flat,
-                               int32_t *flat_count, cudaStream_t st);
+                               int32_t *flat_count, cudaStream_t st,
+                               int32_t *flat_span = nullptr);
+// flat_span (optional): two zeroed ints that receive {INT_MAX - lowest flat
+// window, highest flat window + 1} (both stay 0 without flat windows).
 
 cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const float *mu,
                                     uint8_t *alive, int32_t N, int32_t m, int32_t R,
                                     int32_t max_chunks, float thr_prune,
-                                    const int32_t *flat_count, int32_t *task_counter, int32_t *walked,
-                                    bool with_w, int32_t *status, int32_t num_sms,
+                                    int32_t *task_counter, int32_t *walked, int32_t num_sms,
                                     cudaStream_t st);
 
+// prune_flats (r^2 > 0): flat windows with another flat window at least m-1
+// away are dropped (distance 0); flat_span as filled by paddi_launch_stats.
 cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
                                  uint32_t *rho_max, uint8_t *pruned, int32_t *rc_slot,
-                                 PaddiAttemptDev *att, cudaStream_t st);
+                                 PaddiAttemptDev *att, const uint8_t *flat,
+                                 const int32_t *flat_span, int32_t m, bool prune_flats,
+                                 cudaStream_t st);
 
 // Dense refine of the candidates in list[0..*list_count) (positions into
 // cand[]) against the windows [jb, je).
@@ -154,7 +160,7 @@ cudaError_t paddi_launch_select(const int32_t *cand, PaddiAttemptDev *att,
 
 // with_w: room for the flat-window column data (false only when the length is
 // known to have no flat window).
-size_t paddi_phase1_smem(int R, int m, bool with_w = true);
+size_t paddi_phase1_smem(int R, int m);
 
 cudaError_t paddi_launch_export_stats(const double *mu64, const double *inv64, int32_t N,
                                       int32_t m, float *mean, float *sd, cudaStream_t st);

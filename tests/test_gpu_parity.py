@@ -368,3 +368,37 @@ def test_batched_workload_sample_properties():
         for i in rng.choice(maxL - minL + 1, 2, replace=False):
             d, _ = O.window_nn(x, minL + i, g[i].ind)
             assert abs(g[i].dist - d) <= 1e-5 * d
+
+
+@pytest.mark.parametrize("far_partner", [False, True])
+def test_flat_window_span(ctx, far_partner):
+    """Flat windows with and without an admissible flat partner.
+
+    A flat run of m+5 values gives 6 flat windows, all closer than m-1 to
+    each other: each one's nearest neighbour is a non-flat window at d = 2m,
+    so they lead the discord list.  A second flat run far away gives every
+    flat window a partner at d = 0; those are dropped at candidate compaction.
+    """
+    rng = np.random.default_rng(11)
+    m = 40
+    x = np.cumsum(rng.standard_normal(20000)).astype(np.float32)
+    x[5000:5000 + m + 5] = x[5000]
+    if far_partner:
+        x[15000:15060] = np.float32(-3.0)
+    want, watt = O.pd3(x, m, top_k=3)
+    got, log = ctx.pd3(x, m, top_k=3)
+    assert [d.ind for d in got] == [w[0] for w in want]
+    for d, w in zip(got, want):
+        assert _close(d.dist, w[1])
+    assert [(e["n_cand"], e["n_disc"]) for e in log] == \
+        [(e["n_cand"], e["n_disc"]) for e in watt]
+    # fixed thresholds: a tiny r (inside the guard band of rho = 1), r^2 just
+    # below 2m (the flat windows without a partner stay) and just above it
+    # (flat vs non-flat pairs, d = 2m, prune)
+    nn, _ = O.nn_profile(x, m)
+    for r in (0.05, 1.0, float(np.sqrt(2.0 * m)) - 0.1, float(np.sqrt(2.0 * m)) + 0.5):
+        r2 = float(np.float32(r) * np.float32(r))
+        att, sel = O.select(nn, m, r2, top_k=3)
+        g, lg = ctx.pd3(x, m, top_k=3, r=r)
+        assert (lg[0]["n_cand"], lg[0]["n_disc"]) == (att["n_cand"], att["n_disc"]), r
+        assert [d.ind for d in g] == [s[0] for s in sel], r
