@@ -3,7 +3,7 @@
 //
 // Reference counterparts:
 //   get_node_candidates_num / local_candidates_union (src/sets_processing.hpp:49-113)
-//       -> k_compact: warp-ballot / block-scan compaction of alive windows
+//       -> k_compact: warp-scan / block-scan compaction of alive windows
 //          into an index list, on the device (no host round trip, no copy of
 //          candidate windows: the refine re-reads them from the series);
 //   get_node_discords_num / find_top1_discord (src/sets_processing.hpp:11-87)
@@ -31,47 +31,79 @@ constexpr int RC_THREADS = 256;
 constexpr int RC_MAXM = 1024;
 
 // ---------------------------------------------------------------- compact
+// Each thread tests 16 consecutive windows (one 16-byte load of alive flags);
+// a warp scan and a block scan place them, with one atomicAdd per CTA.
 // With prune_flats (r^2 > 0), a flat window that has another flat window at
 // least m-1 away is no candidate: their distance is exactly 0 < r^2 under the
 // flat-window policy (src/PD3_kernels.cuh:107-108 maps 0/0 to "closer than
 // any r").  Phase 1 leaves flat-flat pairs out (rho 0 there), so this is
 // where such windows are dropped; the span {INT_MAX - lowest, highest + 1}
 // of the flat windows decides it per window.
-__global__ void __launch_bounds__(CP_THREADS)
+constexpr int CP_WIN = 16;                 // windows per thread
+constexpr int CP_CTHREADS = 256;
+__global__ void __launch_bounds__(CP_CTHREADS)
 k_compact(const uint8_t *__restrict__ alive, int32_t N, int32_t *cand, uint32_t *rho_max,
           uint8_t *pruned, int32_t *rc_slot, PaddiAttemptDev *att,
           const uint8_t *__restrict__ flat, const int32_t *__restrict__ flat_span, int32_t m,
           int32_t prune_flats)
 {
-    __shared__ int wcnt[CP_THREADS / 32];
+    __shared__ int wcnt[CP_CTHREADS / 32];
     __shared__ int base;
-    const int i = blockIdx.x * CP_THREADS + threadIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    bool a = i < N && alive[i];
-    if (a && prune_flats && flat[i]) {
-        const int lo = INT_MAX - flat_span[0], hi = flat_span[1] - 1;
-        if (i - lo >= m - 1 || hi - i >= m - 1) a = false;
+    const int i0 = (blockIdx.x * CP_CTHREADS + threadIdx.x) * CP_WIN;
+    uint8_t f[CP_WIN];
+    if (i0 + CP_WIN <= N) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(alive + i0);
+        const uint32_t u[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int b = 0; b < CP_WIN; ++b) f[b] = (u[b >> 2] >> (8 * (b & 3))) & 0xffu;
+    } else {
+#pragma unroll
+        for (int b = 0; b < CP_WIN; ++b) f[b] = i0 + b < N ? alive[i0 + b] : 0;
     }
-    const unsigned b = __ballot_sync(0xffffffffu, a);
-    if (lane == 0) wcnt[w] = __popc(b);
+    uint32_t mask = 0;
+    int lo = 0, hi = -1;
+    if (prune_flats) {
+        lo = INT_MAX - flat_span[0];
+        hi = flat_span[1] - 1;
+    }
+#pragma unroll
+    for (int b = 0; b < CP_WIN; ++b) {
+        bool a = f[b] != 0;
+        const int i = i0 + b;
+        if (a && prune_flats && flat[i] && (i - lo >= m - 1 || hi - i >= m - 1)) a = false;
+        mask |= (uint32_t)a << b;
+    }
+    const int cnt = __popc(mask);
+    int inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) wcnt[w] = inc;
     __syncthreads();
     if (w == 0) {
-        int v = wcnt[lane], inc = v;
+        const int v = lane < CP_CTHREADS / 32 ? wcnt[lane] : 0;
+        int wi = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += t;
+            const int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
         }
-        wcnt[lane] = inc - v;
-        if (lane == 31) base = inc ? atomicAdd(&att->n_cand_p1, inc) : 0;
+        if (lane < CP_CTHREADS / 32) wcnt[lane] = wi - v;
+        if (lane == 31) base = wi ? atomicAdd(&att->n_cand_p1, wi) : 0;
     }
     __syncthreads();
-    if (a) {
-        const int pos = base + wcnt[w] + __popc(b & ((1u << lane) - 1u));
-        cand[pos] = i;
+    int pos = base + wcnt[w] + inc - cnt;
+    while (mask) {
+        const int b = __ffs(mask) - 1;
+        mask &= mask - 1;
+        cand[pos] = i0 + b;
         rho_max[pos] = f2ord(-INFINITY);
         pruned[pos] = 0;
         rc_slot[pos] = -1;
+        ++pos;
     }
 }
 
@@ -556,8 +588,9 @@ cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
                                  const int32_t *flat_span, int32_t m, bool prune_flats,
                                  cudaStream_t st)
 {
-    const unsigned grid = (unsigned)((N + CP_THREADS - 1) / CP_THREADS);
-    k_compact<<<grid, CP_THREADS, 0, st>>>(alive, N, cand, rho_max, pruned, rc_slot, att, flat,
+    const int per_cta = CP_CTHREADS * CP_WIN;
+    const unsigned grid = (unsigned)((N + per_cta - 1) / per_cta);
+    k_compact<<<grid, CP_CTHREADS, 0, st>>>(alive, N, cand, rho_max, pruned, rc_slot, att, flat,
                                            flat_span, m, prune_flats ? 1 : 0);
     return cudaGetLastError();
 }

@@ -77,12 +77,10 @@ struct paddi_ctx {
     float *d_pn = nullptr;
     uint16_t *d_bq = nullptr; // tensor-core refine: split series slices per tile block
     float4 *d_wdq = nullptr;  // tensor-core refine: epilogue window data per tile block
-    // single-window exact nn (r guidance): a one-entry candidate list
-    PaddiAttemptDev *d_att1 = nullptr;
-    int32_t *d_one = nullptr;               // [0] = window, [1] = 0 (recheck slot)
-    unsigned long long *d_nn1 = nullptr;
-    int32_t *h_one = nullptr;               // pinned staging
-    unsigned long long *h_nn1 = nullptr;
+    // r guidance: exact FP64 nn of the bound window, kept incrementally
+    PaddiGuide *d_guide = nullptr, *h_guide = nullptr; // state + result (h: pinned)
+    double *d_G = nullptr;                  // shifted dot products, two buffers (on first use)
+    size_t G_cap = 0;                       // windows per buffer
     int32_t *h_flatcount = nullptr;         // pinned
     // learned r predictor
     bool model_ok = false;
@@ -154,6 +152,8 @@ void free_buffers(paddi_ctx *ctx)
     dfree(ctx->d_wdq);
     dfree(ctx->d_pc);
     dfree(ctx->d_pn);
+    dfree(ctx->d_G);
+    ctx->G_cap = 0;
     ctx->cap_n = 0;
     ctx->rc_cap = 0;
 }
@@ -233,10 +233,19 @@ paddi_status run_stats(paddi_ctx *ctx, const float *x, size_t n, int m, bool til
 
 // One (m, r2) attempt on the statistics currently in the context.
 // known_w >= 0: window whose exact FP64 nn at this length is already known
-// (its ordered image known_ord, from window_nn64); the recheck skips it.
+// (its ordered image known_ord, from the guide kernel); the recheck skips it.
+paddi_status enqueue_prep(paddi_ctx *ctx, const float *x, size_t n, int m, bool guided,
+                          int32_t w_host);
+
+// next_m > 0: the statistics (and, with next_guided, the bound) of length
+// next_m are queued behind the attempt, before its result is synced, so the
+// host waits once per length; *spec_out then tells whether the statistics
+// now hold next_m (not when the selection had to be redone).
 paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float r2, int top_k,
-                         AttemptOut *out, int32_t known_w = -1, unsigned long long known_ord = 0)
+                         AttemptOut *out, int32_t known_w = -1, unsigned long long known_ord = 0,
+                         int next_m = 0, bool next_guided = false, bool *spec_out = nullptr)
 {
+    bool spec = false;
     const int32_t N = (int32_t)(n - m + 1);
     const int kernel = refine_kernel_for(ctx, m);
     const float guard = guard_of(ctx, kernel);
@@ -331,6 +340,11 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         CK(cudaEventRecord(ctx->ev[3], st));
         CK(cudaMemcpyAsync(ctx->h_res, ctx->d_res, sizeof(PaddiAttemptResult),
                            cudaMemcpyDeviceToHost, st));
+        if (pass == 0 && next_m > 0) {
+            paddi_status s = enqueue_prep(ctx, x, n, next_m, next_guided, -1);
+            if (s != PADDI_OK) return s;
+            spec = true;
+        }
         CK(cudaStreamSynchronize(st));
         if (ctx->h_res->status == 1) {
             // more windows need the exact value than the queue holds: grow it and redo
@@ -346,6 +360,11 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
             widen = 1e30f;
         } else {
             break;
+        }
+        if (spec) { // the redo needs this length's statistics back
+            paddi_status s = run_stats(ctx, x, n, m);
+            if (s != PADDI_OK) return s;
+            spec = false;
         }
         CK(cudaMemsetAsync(&ctx->d_att->recheck_next, 0, sizeof(int32_t), st));
         CK(cudaMemsetAsync(&ctx->d_att->status, 0, sizeof(int32_t), st));
@@ -364,6 +383,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT, "top-k selection did not settle");
     out->res = *ctx->h_res;
     out->launches = launches;
+    if (spec_out) *spec_out = spec;
     if (ctx->trace) {
         std::string line = "paddi-trace m=" + std::to_string(m) + " r2=" + std::to_string(r2) +
                            " p1=" + std::to_string(ctx->h_res->n_p1) +
@@ -421,33 +441,66 @@ bool valid_lengths(size_t n, uint32_t minL, uint32_t maxL)
            n < (size_t)INT32_MAX - PADDI_PAD_WIN - 64;
 }
 
-// Exact FP64 nearest-neighbour distance of window w at the length whose
-// statistics are current (the FP64 recheck kernel with a one-entry list).
-paddi_status window_nn64(paddi_ctx *ctx, const float *x, size_t n, int m, int w, double *out)
+// What is known about one length before its first attempt: the timing of
+// its statistics, its flat-window count and, for the guided r policies, the
+// exact FP64 nn of the bound window (the previous length's top-1 window).
+struct Prep {
+    int m = 0;                        // length prepared (0: none)
+    float ms_stats = 0.f, ms_guide = 0.f;
+    int32_t flatcount = 0;
+    int32_t known_w = -1;             // bound window with a finite exact nn (-1: none)
+    unsigned long long known_ord = 0; // its ordered image
+    double lb = 0.0;                  // its nn
+};
+
+// Queues the statistics of length m and, with `guided`, the bound window's
+// exact nn (window w_host; w_host < 0: the top-1 window of the attempt result
+// on the device, so this can be queued before the host has read it).  No
+// sync: read_prep collects the values after the next one.
+paddi_status enqueue_prep(paddi_ctx *ctx, const float *x, size_t n, int m, bool guided,
+                          int32_t w_host)
 {
     const int32_t N = (int32_t)(n - m + 1);
-    cudaStream_t st = ctx->st;
-    // att1 = {n_cand_p1 = 1, counters 0, n_recheck = 1}
-    PaddiAttemptDev a1;
-    std::memset(&a1, 0, sizeof(a1));
-    a1.n_cand_p1 = 1;
-    a1.n_recheck = 1;
-    static_assert(sizeof(PaddiAttemptDev) <= 4 * sizeof(int32_t) + 64, "staging");
-    ctx->h_one[0] = w;
-    ctx->h_one[1] = 0;
-    CK(cudaMemcpyAsync(ctx->d_one, ctx->h_one, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->d_att1, &a1, sizeof(a1), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(ctx->d_nn1, 0xff, sizeof(unsigned long long), st)); // +inf image
-    CK(paddi_launch_recheck(x, ctx->d_mu64, ctx->d_inv64, ctx->d_flat, N, m, ctx->d_one,
-                            ctx->d_one + 1, ctx->d_att1, ctx->d_nn1, ctx->num_sms, -1, st));
-    CK(cudaMemcpyAsync(ctx->h_nn1, ctx->d_nn1, sizeof(unsigned long long),
-                       cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    const unsigned long long u = *ctx->h_nn1;
-    const unsigned long long bits = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
-    double d;
-    std::memcpy(&d, &bits, sizeof(d));
-    *out = d;
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    paddi_status s = run_stats(ctx, x, n, m);
+    if (s != PADDI_OK) return s;
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    CK(cudaMemcpyAsync(ctx->h_flatcount, ctx->d_flatcount, sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    if (guided) {
+        CK(cudaEventRecord(ctx->ev[6], ctx->st));
+        CK(paddi_launch_guide(x, ctx->d_mu64, ctx->d_inv64, ctx->d_flat, N, m, ctx->d_res, w_host,
+                              ctx->d_guide, ctx->d_G, ctx->G_cap, ctx->num_sms, ctx->st));
+        CK(cudaMemcpyAsync(ctx->h_guide, ctx->d_guide, sizeof(PaddiGuide),
+                           cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaEventRecord(ctx->ev[7], ctx->st));
+    }
+    return PADDI_OK;
+}
+
+// After a sync that covers enqueue_prep(m, guided).
+paddi_status read_prep(paddi_ctx *ctx, int m, bool guided, Prep *p)
+{
+    *p = Prep();
+    p->m = m;
+    CK(cudaEventElapsedTime(&p->ms_stats, ctx->ev[4], ctx->ev[5]));
+    p->flatcount = *ctx->h_flatcount;
+    if (guided) {
+        CK(cudaEventElapsedTime(&p->ms_guide, ctx->ev[6], ctx->ev[7]));
+        const unsigned long long u = ctx->h_guide->nn_ord;
+        const unsigned long long bits =
+            (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+        double d;
+        std::memcpy(&d, &bits, sizeof(d));
+        if (ctx->h_guide->w_used >= 0 && std::isfinite(d)) {
+            p->known_w = ctx->h_guide->w_used;
+            p->known_ord = u;
+            p->lb = d;
+        }
+        if (ctx->trace)
+            std::fprintf(stderr, "paddi-guide m=%d w=%d mode=%d ms=%f\n", m,
+                         ctx->h_guide->w_used, ctx->h_guide->mode, p->ms_guide);
+    }
     return PADDI_OK;
 }
 
@@ -565,41 +618,57 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
         out[j].dist = -FLT_MAX;
     }
     int prev_attempts = 0;
+    const bool guided = want_lb || policy == PADDI_R_LEARNED;
+    // with the profile callback every length's statistics must stay current
+    // until its profile is written: no statistics are queued ahead then
+    const bool ahead = guided && !prof_fn;
+    if (guided) {
+        const size_t W = ctx->cap_n + PADDI_PAD_WIN + 64;
+        if (ctx->G_cap < W) {
+            dfree(ctx->d_G);
+            ctx->G_cap = 0;
+            CK(cudaMalloc(&ctx->d_G, sizeof(double) * 2 * W)); // two buffers
+            ctx->G_cap = W;
+        }
+        // the dot products of an earlier call belong to another series
+        CK(cudaMemsetAsync(ctx->d_guide, 0, sizeof(PaddiGuide), ctx->st));
+    }
+    Prep pre; // the length whose statistics (and bound) are current, if queued ahead
     for (int j = 0; j < L; ++j) {
         const int m = (int)minL + j;
         const int32_t N = (int32_t)(n - m + 1);
-        CK(cudaEventRecord(ctx->ev[4], ctx->st));
-        paddi_status s = run_stats(ctx, x, n, m);
-        if (s != PADDI_OK) return s;
-        CK(cudaEventRecord(ctx->ev[5], ctx->st));
-        CK(cudaMemcpyAsync(ctx->h_flatcount, ctx->d_flatcount, sizeof(int32_t),
-                           cudaMemcpyDeviceToHost, ctx->st));
+        paddi_status s;
+        // ---- statistics and the bound: queued ahead by the previous length's
+        //      last attempt, or here (the previous length's top-1 window,
+        //      evaluated exactly at this length: its nn is a lower bound on
+        //      this length's top-1 distance)
+        const bool g_here = guided && j >= 1 && out[j - 1].ind >= 0;
+        bool need_read = false;
+        if (pre.m != m) {
+            const int32_t w = g_here ? (out[j - 1].ind < N ? out[j - 1].ind : N - 1) : -1;
+            s = enqueue_prep(ctx, x, n, m, g_here, w);
+            if (s != PADDI_OK) return s;
+            if (g_here || ahead) { // (queueing ahead re-records the prep events)
+                CK(cudaStreamSynchronize(ctx->st));
+                s = read_prep(ctx, m, g_here, &pre);
+                if (s != PADDI_OK) return s;
+            } else {
+                need_read = true; // read after the first attempt's sync
+            }
+        }
+        Prep cur = pre; // the next length's values may replace pre during the attempts
+        pre.m = 0;
         float S = 0.f;
         float r = merlin_first_r(out, j, minL, &S);
         // ---- guidance: the bound and / or the model's prediction
-        float ms_guide = 0.f, lbf = 0.f, lbm = 0.f; // lbm: largest r^2 below the bound
-        int32_t known_w = -1;           // the bound's window: its exact nn is known
-        unsigned long long known_ord = 0;
+        float lbf = 0.f, lbm = 0.f; // lbm: largest r^2 below the bound
         int source = 0;
-        if (j >= 1 && out[j - 1].ind >= 0 && (want_lb || policy == PADDI_R_LEARNED)) {
-            // the previous length's top-1 window, evaluated exactly at this length:
-            // its nn is a lower bound on this length's top-1 distance
-            const int w = out[j - 1].ind < N ? out[j - 1].ind : N - 1;
-            CK(cudaEventRecord(ctx->ev[6], ctx->st));
-            double lb = 0.0;
-            s = window_nn64(ctx, x, n, m, w, &lb);
-            if (s != PADDI_OK) return s;
-            if (std::isfinite(lb)) {
-                known_w = w;
-                known_ord = *ctx->h_nn1;
-            }
-            if (std::isfinite(lb) && lb > 0.0) {
-                lbf = (float)std::fmin(lb, (double)FLT_MAX);
-                const float rb = r_below(lbf);
-                lbm = rb * rb;
-            }
+        if (!need_read && cur.known_w >= 0 && cur.lb > 0.0) {
+            lbf = (float)std::fmin(cur.lb, (double)FLT_MAX);
+            const float rb = r_below(lbf);
+            lbm = rb * rb;
         }
-        const float flat_frac = (float)*ctx->h_flatcount / (float)N; // synced above when guided
+        const float flat_frac = (float)cur.flatcount / (float)N;
         if (policy == PADDI_R_BOUND && lbm > 0.f && lbm > r * r) {
             // tighter than MERLIN's first r and certain to find a discord (a window
             // that was flat at m-1 may have a small nn at m: then MERLIN leads)
@@ -626,37 +695,45 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
                 source = 1;
             }
         }
-        if (j >= 1 && (want_lb || policy == PADDI_R_LEARNED)) {
-            CK(cudaEventRecord(ctx->ev[7], ctx->st));
-            CK(cudaEventSynchronize(ctx->ev[7]));
-            CK(cudaEventElapsedTime(&ms_guide, ctx->ev[6], ctx->ev[7]));
-        }
         // ---- attempts
         int it = 0;
         bool first = true;
+        bool stale = false; // the statistics hold the next length (queued ahead)
+        bool spec = false;
         while (out[j].dist < 0) {
             if (it++ >= iter_cap)
                 return fail(ctx, PADDI_ERR_ITER_CAP,
                             "length " + std::to_string(m) + ": no discord after " +
                                 std::to_string(iter_cap) + " attempts");
+            if (stale) { // a miss after the next length was queued: restore this one
+                s = run_stats(ctx, x, n, m);
+                if (s != PADDI_OK) return s;
+                stale = false;
+            }
             const float r2 = r * r;
             AttemptOut a;
-            s = run_attempt(ctx, x, n, m, r2, 1, &a, known_w, known_ord);
+            const int next_m = ahead && j + 1 < L ? m + 1 : 0;
+            s = run_attempt(ctx, x, n, m, r2, 1, &a, cur.known_w, cur.known_ord, next_m, guided,
+                            &spec);
             if (s != PADDI_OK) return s;
-            float ms_stats = 0.f;
-            if (first) CK(cudaEventElapsedTime(&ms_stats, ctx->ev[4], ctx->ev[5]));
+            stale = spec;
+            if (need_read) {
+                s = read_prep(ctx, m, false, &cur);
+                if (s != PADDI_OK) return s;
+                need_read = false;
+            }
             if (a.res.n_sel > 0) {
                 out[j].ind = a.res.sel_ind[0];
                 out[j].dist = a.res.sel_dist[0];
             }
             if (log && nl < log_cap) {
-                fill_log(&log[nl], m, r, r2, 1, a, ms_stats);
+                fill_log(&log[nl], m, r, r2, 1, a, first ? cur.ms_stats : 0.f);
                 log[nl].r_source = source;
                 log[nl].lb = lbf;
-                log[nl].flat_frac = (float)*ctx->h_flatcount / (float)N;
+                log[nl].flat_frac = (float)cur.flatcount / (float)N;
                 if (first) {
-                    log[nl].ms_guide = ms_guide;
-                    log[nl].ms_total += ms_guide;
+                    log[nl].ms_guide = cur.ms_guide;
+                    log[nl].ms_total += cur.ms_guide;
                     log[nl].n_launches += (lbf > 0.f ? 1 : 0) + (source == 1 ? 1 : 0);
                 }
             }
@@ -679,6 +756,10 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
                     source = 2;
                 }
             }
+        }
+        if (spec) { // the last attempt queued the next length
+            s = read_prep(ctx, m + 1, guided, &pre);
+            if (s != PADDI_OK) return s;
         }
         prev_attempts = it;
         if (prof_fn) {
@@ -768,11 +849,9 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
     ok = ok && cudaMalloc(&ctx->d_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_flatcount, 3 * sizeof(int32_t)) == cudaSuccess;
     ok = ok && cudaMallocHost(&ctx->h_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
-    ok = ok && cudaMalloc(&ctx->d_att1, sizeof(PaddiAttemptDev)) == cudaSuccess;
-    ok = ok && cudaMalloc(&ctx->d_one, 2 * sizeof(int32_t)) == cudaSuccess;
-    ok = ok && cudaMalloc(&ctx->d_nn1, sizeof(unsigned long long)) == cudaSuccess;
-    ok = ok && cudaMallocHost(&ctx->h_one, 4 * sizeof(int32_t)) == cudaSuccess;
-    ok = ok && cudaMallocHost(&ctx->h_nn1, sizeof(unsigned long long)) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_guide, sizeof(PaddiGuide)) == cudaSuccess;
+    ok = ok && cudaMemset(ctx->d_guide, 0, sizeof(PaddiGuide)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&ctx->h_guide, sizeof(PaddiGuide)) == cudaSuccess;
     ok = ok && cudaMallocHost(&ctx->h_flatcount, sizeof(int32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_model, sizeof(float) * MLP_NPARAM) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_model_bf16, 2 * MLP_NPARAM) == cudaSuccess;
@@ -797,17 +876,14 @@ PADDI_API paddi_status paddi_ctx_destroy(paddi_ctx *ctx)
     dfree(ctx->d_att);
     dfree(ctx->d_res);
     dfree(ctx->d_flatcount);
-    dfree(ctx->d_att1);
-    dfree(ctx->d_one);
-    dfree(ctx->d_nn1);
+    dfree(ctx->d_guide);
     dfree(ctx->d_model);
     if (ctx->d_model_bf16) cudaFree(ctx->d_model_bf16);
     dfree(ctx->d_feat);
     dfree(ctx->d_pred);
     if (ctx->h_feat) cudaFreeHost(ctx->h_feat);
     if (ctx->h_flatcount) cudaFreeHost(ctx->h_flatcount);
-    if (ctx->h_one) cudaFreeHost(ctx->h_one);
-    if (ctx->h_nn1) cudaFreeHost(ctx->h_nn1);
+    if (ctx->h_guide) cudaFreeHost(ctx->h_guide);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);

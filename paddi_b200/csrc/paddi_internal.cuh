@@ -73,6 +73,20 @@ struct PaddiAttemptResult {
     unsigned long long n_pairs; // refine pairs evaluated
 };
 
+// Incremental FP64 nn of the r policy's bound window (k_guide.cu): the state
+// of the shifted dot products G (two buffers), the launch's result, and
+// kernel counters.  A zeroed record holds no state (no length is 0).
+enum { PADDI_GUIDE_SKIPPED = 0, PADDI_GUIDE_REUSED = 1, PADDI_GUIDE_SLID = 2,
+       PADDI_GUIDE_BUILT = 3 };
+struct PaddiGuide {
+    unsigned long long nn_ord; // result: ordered image of the nn (all ones: none)
+    double s;                  // state: shift of both operands of G
+    int32_t w, m;              // state: window and length G holds
+    int32_t cur, age;          // state: buffer holding G, slides since the last build
+    int32_t w_used, mode;      // result: window of the launch (-1: skipped), PADDI_GUIDE_*
+    int32_t done, item;        // kernel counters (zero between launches)
+};
+
 #define PADDI_MAX_TOPK 16
 #define PADDI_MAX_RECHECK 1024 /* initial FP64 recheck capacity (grows on demand) */
 
@@ -161,6 +175,15 @@ cudaError_t paddi_launch_select(const int32_t *cand, PaddiAttemptDev *att,
 // with_w: room for the flat-window column data (false only when the length is
 // known to have no flat window).
 size_t paddi_phase1_smem(int R, int m);
+
+// Exact FP64 nn at length m of window w_host (w_host < 0: the top-1 window
+// of the attempt result `prev`, skipped when it has none), through the shifted
+// dot products (two buffers G of N doubles each, G + g_stride the second) and
+// their state in g; result in g->nn_ord.
+cudaError_t paddi_launch_guide(const float *x, const double *mu64, const double *inv64,
+                               const uint8_t *flat, int32_t N, int32_t m,
+                               const PaddiAttemptResult *prev, int32_t w_host, PaddiGuide *g,
+                               double *G, size_t g_stride, int32_t num_sms, cudaStream_t st);
 
 cudaError_t paddi_launch_export_stats(const double *mu64, const double *inv64, int32_t N,
                                       int32_t m, float *mean, float *sd, cudaStream_t st);

@@ -295,6 +295,35 @@ def test_r_policy_gives_the_same_discords(policy):
     assert guided and all(e["found"] for e in guided)
 
 
+
+def test_bound_is_the_exact_nn_of_the_previous_top_window():
+    """The bound of every guided length is the exact FP64 nn, at that length,
+    of the previous length's top-1 window.  On this series the top-1 window
+    stays, moves by one or two places and jumps between anomalies, so the
+    incremental dot products are reused, slid and rebuilt; a run on another
+    series first must leave no state behind."""
+    x = _series(8192, 5, "palmad")
+    other = _series(8192, 6, "palmad")
+    minL, maxL = 40, 70
+    with P.Context(r_policy=P.R_BOUND) as c:
+        c.palmad(other, minL, maxL)
+        got, log = c.palmad(x, minL, maxL)
+    want, _ = O.palmad(x, minL, maxL)
+    assert [d.ind for d in got] == [w[0] for w in want]
+    first = {}
+    for e in log:
+        first.setdefault(e["m"], e)
+    checked = 0
+    for m in range(minL + 1, maxL + 1):
+        N = len(x) - m + 1
+        w = min(got[m - 1 - minL].ind, N - 1)
+        nn, _ = O.window_nn(x, m, w)
+        lb = first[m]["lb"]
+        if lb > 0:
+            assert abs(lb - float(np.float32(nn))) <= 1e-6 * nn, (m, w, lb, nn)
+            checked += 1
+    assert checked >= maxL - minL - 2
+
 # ------------------------------------------------------------- batched series
 def test_batched_uneven_series_match_single_runs(ctx):
     series = [x for x, _ in datagen.batch_series(count=6, seed=3, min_log2=12, max_log2=13,
