@@ -52,7 +52,8 @@ constexpr int GD_SPAN = GD_THREADS * GD_JPT;       // windows per build item
 constexpr int GD_MAXM = 1024;
 constexpr int GD_MAX_AGE = 64;                     // slides before a rebuild
 constexpr int GD_MAX_SLIDE = 32;                   // largest |delta| of a slide
-constexpr int GD_STREAM_CTAS_PER_SM = 8;
+constexpr int GD_STREAM_CTAS_PER_SM = 4;          // one wave at <= 64 registers
+constexpr int GD_UNROLL = 4;                       // windows per thread and step (stream)
 
 __device__ __forceinline__ int gpad(int d) { return d + (d >> 4); } // conflict-free at stride 8
 
@@ -135,7 +136,7 @@ __device__ __forceinline__ void guide_finish(double best, double *red, PaddiGuid
 }
 
 // Reuse and slide.  Leaves without a trace when a rebuild is due.
-__global__ void __launch_bounds__(GD_THREADS)
+__global__ void __launch_bounds__(GD_THREADS, GD_STREAM_CTAS_PER_SM)
 k_guide_stream(const float *__restrict__ x, const double *__restrict__ mu64,
                const double *__restrict__ inv64, const uint8_t *__restrict__ flat, int32_t N,
                int32_t m, const PaddiAttemptResult *__restrict__ prev, int32_t w_host,
@@ -143,6 +144,7 @@ k_guide_stream(const float *__restrict__ x, const double *__restrict__ mu64,
 {
     __shared__ double redm[GD_THREADS / 32];
     __shared__ double cf[2 * GD_MAX_SLIDE + 2]; // slide coefficients, signed
+    __shared__ int coff[2 * GD_MAX_SLIDE + 2];  // their partner offsets (from j)
     const int t = threadIdx.x;
     const int w = guide_window(prev, w_host, N);
     if (w < 0) { // no top-1 window: nothing to bound with, the state stays
@@ -168,7 +170,8 @@ k_guide_stream(const float *__restrict__ x, const double *__restrict__ mu64,
     //      ranges overlap (|delta| < m), so the terms are the values between
     //      the two starts, [f0, f0+nf) (added when w < gw, else removed), and
     //      between the two ends, [e0, e0+ne) (added when the new end is
-    //      later); their signed, shifted values go to cf
+    //      later); their signed, shifted values go to cf, their offsets
+    //      from the partner window's start to coff
     int nf = 0, ne = 0, f0 = 0, e0 = 0;
     int blo = 0, bhi = N; // windows without an old partner entry: [0, blo) and [bhi, N)
     if (mode == PADDI_GUIDE_SLID) {
@@ -179,8 +182,11 @@ k_guide_stream(const float *__restrict__ x, const double *__restrict__ mu64,
         e0 = min(a1, b1);
         ne = max(a1, b1) - e0;
         const double es = a1 > b1 ? 1.0 : -1.0;
-        for (int k = t; k < nf + ne; k += GD_THREADS)
-            cf[k] = k < nf ? fs * ((double)x[f0 + k] - s) : es * ((double)x[e0 + k - nf] - s);
+        for (int k = t; k < nf + ne; k += GD_THREADS) {
+            const int q = k < nf ? f0 + k : e0 + k - nf;
+            cf[k] = (k < nf ? fs : es) * ((double)x[q] - s);
+            coff[k] = q - w;
+        }
         blo = delta > 0 ? delta : 0;
         bhi = min(N, N + 1 + delta); // old entries exist for j - delta < N + 1
         // windows without an old entry: direct sums, one per CTA
@@ -197,24 +203,45 @@ k_guide_stream(const float *__restrict__ x, const double *__restrict__ mu64,
                 best = fmin(best, pair_dist(cov, iw, inv64[jj], fw, flat[jj], m));
             }
         }
-        __syncthreads(); // cf staged
     }
-    // ---- streaming pass over the windows with an old entry
+    __syncthreads(); // cf, coff staged
+    // ---- streaming pass over the windows with an old entry: GD_UNROLL
+    //      windows a stride apart per thread and step, their loads issued
+    //      together (the pass is bound by load latency, not bandwidth)
     const int stride = gridDim.x * GD_THREADS;
-    for (int j = blo + blockIdx.x * GD_THREADS + t; j < bhi; j += stride) {
-        double gj;
-        if (mode == PADDI_GUIDE_SLID) {
-            gj = Gin[j - delta];
-            const float *xf = x + j + (f0 - w), *xe = x + j + (e0 - w);
-            for (int k = 0; k < nf; ++k) gj = fma(cf[k], (double)xf[k] - s, gj);
-            for (int k = 0; k < ne; ++k) gj = fma(cf[nf + k], (double)xe[k] - s, gj);
-            Gout[j] = gj;
-        } else {
-            gj = Gin[j];
+    const int nt = nf + ne;
+    const int shift = mode == PADDI_GUIDE_SLID ? delta : 0;
+    for (int j0 = blo + blockIdx.x * GD_THREADS + t; j0 < bhi; j0 += GD_UNROLL * stride) {
+        double gv[GD_UNROLL], mv[GD_UNROLL], iv[GD_UNROLL];
+        int fv[GD_UNROLL];
+#pragma unroll
+        for (int u = 0; u < GD_UNROLL; ++u) {
+            const int j = j0 + u * stride;
+            const bool ok = j < bhi;
+            gv[u] = ok ? Gin[j - shift] : 0.0;
+            mv[u] = ok ? mu64[j] : 0.0;
+            iv[u] = ok ? inv64[j] : 0.0;
+            fv[u] = ok ? flat[j] : 0;
         }
-        if (admissible(w, j, m)) {
-            const double cov = gj - cw * (mu64[j] - s);
-            best = fmin(best, pair_dist(cov, iw, inv64[j], fw, flat[j], m));
+        for (int k = 0; k < nt; ++k) {
+            const double c = cf[k];
+            const int o = coff[k];
+#pragma unroll
+            for (int u = 0; u < GD_UNROLL; ++u) {
+                const int j = j0 + u * stride;
+                if (j < bhi) gv[u] = fma(c, (double)x[j + o] - s, gv[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < GD_UNROLL; ++u) {
+            const int j = j0 + u * stride;
+            if (j < bhi) {
+                if (mode == PADDI_GUIDE_SLID) Gout[j] = gv[u];
+                if (admissible(w, j, m)) {
+                    const double cov = gv[u] - cw * (mv[u] - s);
+                    best = fmin(best, pair_dist(cov, iw, iv[u], fw, fv[u], m));
+                }
+            }
         }
     }
     const bool slid = mode == PADDI_GUIDE_SLID;
