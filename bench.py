@@ -50,7 +50,7 @@ CPU_SAMPLE_LENGTHS = 8          # lengths 64..71
 L2_FLUSH_BYTES = 512 << 20      # > 126 MB L2
 # DRAM bytes (read + write) of one k_refine_umma launch from an ncu capture:
 # the last refine round (windows N/2..N) of an m=300 attempt on this series
-REFINE_TRAFFIC_BYTES = 13463808
+REFINE_TRAFFIC_BYTES = 13450752
 REFINE_TRAFFIC_LAUNCH = "refine round over windows N/2..N at m=300, ncu dram__bytes_read+write"
 
 

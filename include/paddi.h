@@ -66,7 +66,9 @@ typedef enum paddi_r_policy {
     PADDI_R_BOUND = 2     /* first try r^2 just below the exact nn, at this length, of the
                              previous length's top-1 window (a lower bound on this
                              length's top-1 distance, so the try always succeeds);
-                             MERLIN as fallback */
+                             MERLIN as fallback.  BOUND and LEARNED keep the bound's
+                             FP64 dot products resident between lengths: the context
+                             allocates 16 bytes per window on its first guided call */
 } paddi_r_policy;
 
 typedef struct paddi_opts {
