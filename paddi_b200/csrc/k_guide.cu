@@ -23,19 +23,18 @@
 // with direct dot products after 64 slides, when the window moves further,
 // and when the state belongs to another length.
 //
-// One kernel serves every length.  It reads the window (from the host, or
-// from the previous attempt's result on the device, so it can be queued
-// before the host has seen that result), compares it with the state of G and
-// then reuses G (same window and length), slides it into the other buffer, or
-// rebuilds it.  Two kernels are queued per length: k_guide_stream (reuse and
-// slide: a streaming pass with no large shared memory, so it runs at full
-// occupancy) and then k_guide_build (direct dot products, staged in shared
-// memory).  The first decides from the old state; the second acts only if
-// the state was left untouched, i.e. when the first found a rebuild due.
-// Windows whose old partner entry does not exist (|delta| at most, at the
-// ends of the series) are summed directly, one per CTA.  In each kernel the
-// last CTA to finish publishes the new state, after every CTA has read the
-// old one.
+// Two kernels are queued per length.  Both read the window (from the host,
+// or from the previous attempt's result on the device, so they can be queued
+// before the host has seen that result) and compare it with the state of G.
+// k_guide_stream reuses G (same window and length) or slides it into the
+// other buffer: a streaming pass with no large shared memory, four windows
+// per thread and step so their loads are in flight together.  k_guide_build
+// then rebuilds G with direct dot products staged in shared memory, but only
+// if the state was left untouched, i.e. when the first kernel found a
+// rebuild due.  Windows whose old partner entry does not exist (|delta| at
+// most, at the ends of the series) are summed directly, one per CTA.  In
+// each kernel the last CTA to finish publishes the new state, after every
+// CTA has read the old one.
 #include <float.h>
 
 #include <algorithm>
