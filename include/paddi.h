@@ -76,7 +76,8 @@ typedef struct paddi_opts {
     int32_t device;           /* CUDA device ordinal */
     int32_t distance_kernel;  /* paddi_distance_kernel */
     int32_t r_policy;         /* paddi_r_policy */
-    uint32_t segment_len;     /* phase-1 rows per segment (reference SEGMENT_N); 0 = 256 */
+    uint32_t segment_len;     /* phase-1 rows per segment (reference SEGMENT_N); 0 = 256,
+                                 else 64..4096 (others: PADDI_ERR_UNSUPPORTED) */
     uint32_t phase1_chunks;   /* 256-diagonal chunks a segment scans before the refine; 0 = 12 */
     uint32_t iter_cap;        /* attempts allowed per length; 0 = 200 */
     float guard;              /* correlation guard band of the FP32/BF16 decisions; 0 = default */
@@ -140,6 +141,8 @@ paddi_status paddi_ctx_reserve(paddi_ctx *ctx, size_t n, uint32_t maxL);
  *           top_k non-overlapping discords exist (the reference's first-length
  *           loop, src/main.cu:136-156, with the top-k condition of :137).
  * series: host pointer to n float32 values.  top_k in [1, 16].
+ * segment_len: phase-1 rows per segment, 0 (the context's) or 64..4096;
+ *   other values return PADDI_ERR_UNSUPPORTED.  Results do not depend on it.
  * log (optional) receives one row per attempt, at most log_cap rows.
  */
 paddi_status paddi_pd3(paddi_ctx *ctx, const float *series, size_t n, uint32_t m,
@@ -262,6 +265,26 @@ paddi_status paddi_model_grad(paddi_ctx *ctx, const float *X, const float *Y, ui
 paddi_status paddi_model_predict(paddi_ctx *ctx, const float *X, uint32_t n,
                                  const float *params, int32_t bf16, float *Y);
 
+/* ------------------------------------------------------------------ test hooks
+ * No counterpart in the reference, which exits the process on any CUDA error
+ * (src/common.h:6-16).  These make a failure happen on the host, or make a
+ * bounded device wait run out, so tests can check that the error reaches the
+ * caller as a status and that the context stays usable afterwards.  Nothing
+ * faults the GPU: the refine's waits all have a limit, after which the kernel
+ * records the timeout, waits (bounded) for its own copies and MMAs, frees its
+ * tensor memory and returns. */
+typedef enum paddi_debug_key {
+    PADDI_DEBUG_FAIL_ALLOC = 1,     /* value k > 0: the k-th next device allocation of the
+                                       context fails (PADDI_ERR_OUT_OF_MEMORY); 0: off */
+    PADDI_DEBUG_WAIT_CYCLES = 2,    /* limit of the refine's barrier waits in clock cycles
+                                       (0: the default, about 2 s) */
+    PADDI_DEBUG_WITHHOLD_STAGE = 3, /* 1: the next tensor-core refine launches never fill one
+                                       pipeline stage, so a wait runs out (PADDI_ERR_CUDA) */
+    PADDI_DEBUG_LAST_PASSES = 4     /* read only: selection passes of the last attempt */
+} paddi_debug_key;
+paddi_status paddi_debug_set(paddi_ctx *ctx, int32_t key, int64_t value);
+paddi_status paddi_debug_get(paddi_ctx *ctx, int32_t key, int64_t *value);
+
 /* Largest window count (n - m + 1) that paddi_compute_statistics_noalloc accepts. */
 #define PADDI_NOALLOC_MAX_WINDOWS 131072
 
@@ -279,7 +302,9 @@ paddi_status paddi_model_predict(paddi_ctx *ctx, const float *X, uint32_t n,
  *   - Limit: n - m + 1 <= PADDI_NOALLOC_MAX_WINDOWS, 3 <= m <= 1024, n >= 2m;
  *     anything else returns PADDI_ERR_INVALID_ARG and enqueues nothing.
  *   - The first call on a device looks up the scratch address; make it
- *     before any stream capture begins on that device.
+ *     before any stream capture begins on that device.  Calls that are not
+ *     under capture look it up again, so the entry point stays valid after
+ *     cudaDeviceReset or from another context of the device.
  *   - All calls on a device share the scratch: calls whose GPU work overlaps
  *     (different streams or host threads) race; run them one after another.
  */

@@ -237,6 +237,216 @@ OR_EXPORT void or_nn_profile(const float *x, int64_t n, int32_t m, int32_t right
     series_free(&s);
 }
 
+/*
+ * nn[i] = min over admissible j (|i - j| >= m-1) of d(i, j), FP64, for long
+ * series: the same diagonal recurrence as or_nn_profile method 1, over blocks
+ * of 8 neighbouring diagonals so the inner loop vectorises, re-anchored by a
+ * direct dot product every 8192 rows (the FP64 recurrence drifts by ~1e-12 of
+ * n_i n_j over that many steps).  Pairs with a flat window get d = 2m in the
+ * loop; flat windows are settled afterwards by the flat-window rule (d = 0 to
+ * any admissible flat window).  Windows without an admissible neighbour get
+ * +inf.  Only nn is returned (no index).
+ */
+#define PB_D 8
+#define PB_ANCHOR 8192
+OR_EXPORT void or_nn_profile_fast(const float *x, int64_t n, int32_t m, double *nn)
+{
+    or_series s;
+    series_init(&s, x, n, m);
+    const int64_t N = s.N;
+    const int32_t gap = m - 1;
+    int nth = 1;
+#ifdef _OPENMP
+    nth = omp_get_max_threads();
+#endif
+    double *tnn = (double *)malloc(sizeof(double) * (size_t)(N + PB_D) * nth);
+    for (int64_t k = 0; k < (N + PB_D) * nth; ++k) tnn[k] = INFINITY;
+    double *df = (double *)calloc((size_t)(N + PB_D), sizeof(double));
+    double *dg = (double *)calloc((size_t)(N + PB_D), sizeof(double));
+    double *iv = (double *)calloc((size_t)(N + PB_D), sizeof(double));
+    for (int64_t i = 0; i + 1 < N; ++i) {
+        df[i] = ((double)x[i + m] - (double)x[i]) * 0.5;
+        dg[i] = ((double)x[i + m] - s.mu[i + 1]) + ((double)x[i] - s.mu[i]);
+    }
+    for (int64_t i = 0; i < N; ++i) iv[i] = s.inv[i];
+    const double twom = 2.0 * m;
+    const int64_t nblk = N > gap ? (N - gap + PB_D - 1) / PB_D : 0;
+#pragma omp parallel
+    {
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        double *mnn = tnn + (size_t)t * (N + PB_D);
+#pragma omp for schedule(dynamic, 4)
+        for (int64_t b = 0; b < nblk; ++b) {
+            const int64_t d0 = gap + b * PB_D;
+            double cov[PB_D];
+            /* rows i with i + d0 + PB_D - 1 < N: all 8 diagonals in range */
+            const int64_t full = N - (d0 + PB_D - 1);
+            for (int64_t i0 = 0; i0 < full; i0 += PB_ANCHOR) {
+                const int64_t i1 = i0 + PB_ANCHOR < full ? i0 + PB_ANCHOR : full;
+                for (int k = 0; k < PB_D; ++k) cov[k] = cov_direct(&s, i0, i0 + d0 + k);
+                for (int64_t i = i0; i < i1; ++i) {
+                    const double ivi = iv[i], dfi = df[i], dgi = dg[i];
+                    const int64_t j = i + d0;
+                    double rmin = mnn[i];
+#pragma omp simd reduction(min : rmin)
+                    for (int k = 0; k < PB_D; ++k) {
+                        double d = twom * (1.0 - cov[k] * ivi * iv[j + k]);
+                        d = d < 0.0 ? 0.0 : d;
+                        rmin = d < rmin ? d : rmin;
+                        mnn[j + k] = d < mnn[j + k] ? d : mnn[j + k];
+                        cov[k] += dfi * dg[j + k] + df[j + k] * dgi;
+                    }
+                    mnn[i] = rmin;
+                }
+            }
+            /* the triangle at the end: diagonal d0 + k has N - d0 - k rows */
+            for (int k = 0; k < PB_D; ++k) {
+                const int64_t d = d0 + k;
+                if (d >= N) break;
+                const int64_t i_lo = full > 0 ? full : 0;
+                if (i_lo + d >= N) continue;
+                double c = cov_direct(&s, i_lo, i_lo + d);
+                for (int64_t i = i_lo; i + d < N; ++i) {
+                    const int64_t j = i + d;
+                    double dd = twom * (1.0 - c * iv[i] * iv[j]);
+                    dd = dd < 0.0 ? 0.0 : dd;
+                    if (dd < mnn[i]) mnn[i] = dd;
+                    if (dd < mnn[j]) mnn[j] = dd;
+                    if (j + 1 < N) c += df[i] * dg[j] + df[j] * dg[i];
+                }
+            }
+        }
+    }
+    int64_t flo = -1, fhi = -1;
+    for (int64_t i = 0; i < N; ++i)
+        if (s.flat[i]) {
+            if (flo < 0) flo = i;
+            fhi = i;
+        }
+    for (int64_t i = 0; i < N; ++i) {
+        double b = INFINITY;
+        for (int t = 0; t < nth; ++t) {
+            const double d = tnn[(size_t)t * (N + PB_D) + i];
+            if (d < b) b = d;
+        }
+        if (s.flat[i] && (i - flo >= gap || fhi - i >= gap)) b = 0.0;
+        nn[i] = b;
+    }
+    free(tnn);
+    free(df);
+    free(dg);
+    free(iv);
+    series_free(&s);
+}
+
+/* nn of many windows (FP64, direct dot products, GPU exclusion rule), in
+ * parallel over the windows: out[q] = nn of window w[q], arg[q] its nearest
+ * neighbour (lowest index on ties).  Statistics are computed once. */
+OR_EXPORT void or_windows_nn(const float *x, int64_t n, int32_t m, const int64_t *w,
+                             int64_t count, double *out, int64_t *arg)
+{
+    or_series s;
+    series_init(&s, x, n, m);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t q = 0; q < count; ++q) {
+        const int64_t i = w[q];
+        double best = INFINITY;
+        int64_t bj = -1;
+        for (int64_t j = 0; j < s.N; ++j) {
+            const int64_t dd = i > j ? i - j : j - i;
+            if (dd < m - 1) continue;
+            const double d = dist_from_cov(&s, i, j, cov_direct(&s, i, j));
+            if (d < best) {
+                best = d;
+                bj = j;
+            }
+        }
+        out[q] = best;
+        if (arg) arg[q] = bj;
+    }
+    series_free(&s);
+}
+
+/*
+ * out[L] = FP64 nn at length minL + L of window w[L] (one window per length,
+ * e.g. the reported top-1 of every length of a PALMAD run), in parallel over
+ * the lengths.  The statistics of a length come from long-double prefix sums
+ * of the series shifted by its first value (O(N), relative error ~1e-16 of
+ * the window's own energy for the series of the tests); flatness is the exact
+ * run test.  The dot products are direct and centred on both sides.
+ */
+OR_EXPORT void or_lengths_nn(const float *x, int64_t n, int32_t minL, int32_t maxL,
+                             const int64_t *w, double *out)
+{
+    const int32_t L = maxL - minL + 1;
+    long double *p1 = (long double *)malloc(sizeof(long double) * (size_t)(n + 1));
+    long double *p2 = (long double *)malloc(sizeof(long double) * (size_t)(n + 1));
+    int64_t *runs = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+    const long double c = (long double)x[0];
+    p1[0] = p2[0] = 0.0L;
+    for (int64_t i = 0; i < n; ++i) {
+        const long double d = (long double)x[i] - c;
+        p1[i + 1] = p1[i] + d;
+        p2[i + 1] = p2[i] + d * d;
+    }
+    runs[n - 1] = 1;
+    for (int64_t i = n - 2; i >= 0; --i) runs[i] = (x[i] == x[i + 1]) ? runs[i + 1] + 1 : 1;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int32_t q = 0; q < L; ++q) {
+        const int32_t m = minL + q;
+        const int64_t N = n - m + 1;
+        const int64_t i = w[q];
+        if (i < 0 || i >= N) {
+            out[q] = NAN;
+            continue;
+        }
+        double *mu = (double *)malloc(sizeof(double) * (size_t)N);
+        double *inv = (double *)malloc(sizeof(double) * (size_t)N);
+        uint8_t *fl = (uint8_t *)malloc((size_t)N);
+        for (int64_t j = 0; j < N; ++j) {
+            const long double s1 = p1[j + m] - p1[j], s2 = p2[j + m] - p2[j];
+            const long double u = s1 / m;
+            long double v = s2 - s1 * u;
+            fl[j] = runs[j] >= m;
+            mu[j] = fl[j] ? (double)x[j] : (double)(c + u);
+            if (v < 0.0L) v = 0.0L;
+            inv[j] = (fl[j] || v == 0.0L) ? 0.0 : (double)(1.0L / sqrtl(v));
+            if (inv[j] == 0.0) fl[j] = 1;
+        }
+        double *a = (double *)malloc(sizeof(double) * (size_t)m);
+        for (int32_t k = 0; k < m; ++k) a[k] = (double)x[i + k] - mu[i];
+        double best = INFINITY;
+        for (int64_t j = 0; j < N; ++j) {
+            const int64_t dd = i > j ? i - j : j - i;
+            if (dd < m - 1) continue;
+            double rho;
+            if (fl[i] | fl[j]) {
+                rho = (fl[i] & fl[j]) ? 1.0 : 0.0;
+            } else {
+                const float *b = x + j;
+                const double ub = mu[j];
+                double acc = 0.0;
+                for (int32_t k = 0; k < m; ++k) acc += a[k] * ((double)b[k] - ub);
+                rho = acc * inv[i] * inv[j];
+            }
+            double d = 2.0 * m * (1.0 - rho);
+            d = d < 0.0 ? 0.0 : d;
+            if (d < best) best = d;
+        }
+        out[q] = best;
+        free(a);
+        free(mu);
+        free(inv);
+        free(fl);
+    }
+    free(p1);
+    free(p2);
+    free(runs);
+}
+
 /* nn of a single window (FP64, direct), GPU exclusion rule. */
 OR_EXPORT double or_window_nn(const float *x, int64_t n, int32_t m, int64_t i, int64_t *arg)
 {
@@ -414,12 +624,14 @@ OR_EXPORT int64_t or_palmad(const float *x, int64_t n, int32_t minL, int32_t max
  */
 OR_EXPORT int32_t or_pd3(const float *x, int64_t n, int32_t m, int32_t top_k,
                          int32_t iter_cap, or_discord *sel, or_attempt *log,
-                         int64_t log_cap, int64_t *n_att)
+                         int64_t log_cap, int64_t *n_att, int32_t fast)
 {
     const int64_t N = n - m + 1;
     double *nn = (double *)malloc(sizeof(double) * (size_t)N);
     int64_t *ix = (int64_t *)malloc(sizeof(int64_t) * (size_t)N);
-    or_nn_profile(x, n, m, m - 1, m - 1, 1, nn, ix);
+    /* fast: the vectorised profile re-anchored every 8192 rows (long series) */
+    if (fast) or_nn_profile_fast(x, n, m, nn);
+    else or_nn_profile(x, n, m, m - 1, m - 1, 1, nn, ix);
     float r = (float)(2.0 * sqrt((double)(unsigned)m));
     int64_t na = 0;
     int32_t ns = 0;

@@ -16,6 +16,11 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# The reference's source tree (only its src/cpu_kernels/cpu_kernels.cpp is
+# compiled, into _ref/): PADDI_REF_SRC, else a PADDi checkout beside this
+# repository.  Machines without it use the prebuilt library only.
+REF_SRC = os.environ.get("PADDI_REF_SRC",
+                         os.path.join(os.path.dirname(HERE), "..", "reference", "src"))
 _LIB = None
 _REF = None
 
@@ -39,8 +44,13 @@ class Attempt(C.Structure):
 
 def build() -> None:
     """Compile the checkers (the reference part only where its sources exist)."""
-    target = "all" if os.path.isdir("/root/reference/src") else os.path.join(HERE, "liboracle.so")
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    target = "all" if has_ref_src() else os.path.join(HERE, "liboracle.so")
+    subprocess.run(["make", "-s", "-C", HERE, target, f"REF_SRC={os.path.abspath(REF_SRC)}"],
+                   check=True)
+
+
+def has_ref_src() -> bool:
+    return os.path.isfile(os.path.join(REF_SRC, "cpu_kernels", "cpu_kernels.cpp"))
 
 
 def lib():
@@ -68,8 +78,11 @@ def lib():
         L.or_palmad.restype = C.c_int64
         L.or_pd3.argtypes = [f32p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
                              C.POINTER(Discord), C.POINTER(Attempt), C.c_int64,
-                             C.POINTER(C.c_int64)]
+                             C.POINTER(C.c_int64), C.c_int32]
+        L.or_lengths_nn.argtypes = [f32p, C.c_int64, C.c_int32, C.c_int32, i64p, f64p]
         L.or_pd3.restype = C.c_int32
+        L.or_nn_profile_fast.argtypes = [f32p, C.c_int64, C.c_int32, f64p]
+        L.or_windows_nn.argtypes = [f32p, C.c_int64, C.c_int32, i64p, C.c_int64, f64p, i64p]
         _LIB = L
     return _LIB
 
@@ -80,7 +93,7 @@ def ref():
     if _REF is None:
         p = os.path.join(HERE, "_ref", "libpaddi_ref.so")
         if not os.path.exists(p):
-            if os.path.isdir("/root/reference/src"):
+            if has_ref_src():
                 build()
             else:
                 return None
@@ -130,6 +143,42 @@ def nn_profile(x, m, right_gap=None, left_gap=None, method=1):
     return nn, idx
 
 
+def nn_profile_fast(x, m):
+    """FP64 squared nn distance of every window (no index), for long series:
+    vectorised diagonal blocks re-anchored every 8192 rows."""
+    x = _f32(x)
+    nn = np.empty(len(x) - m + 1, np.float64)
+    lib().or_nn_profile_fast(x, len(x), m, nn)
+    return nn
+
+
+def windows_nn(x, m, windows):
+    """FP64 nn (and nearest index) of each window in ``windows``, in parallel."""
+    x = _f32(x)
+    w = np.ascontiguousarray(windows, dtype=np.int64)
+    out = np.empty(len(w), np.float64)
+    arg = np.empty(len(w), np.int64)
+    lib().or_windows_nn(x, len(x), m, w, len(w), out, arg)
+    return out, arg
+
+
+def lengths_nn(x, minL, maxL, windows):
+    """FP64 nn at length minL + q of window windows[q], for every q, in parallel."""
+    x = _f32(x)
+    w = np.ascontiguousarray(windows, dtype=np.int64)
+    assert len(w) == maxL - minL + 1
+    out = np.empty(len(w), np.float64)
+    lib().or_lengths_nn(x, len(x), minL, maxL, w, out)
+    return out
+
+
+def top1(nn):
+    """(index, float distance) of the PALMAD top-1: the first maximum of float(nn)."""
+    f = np.asarray(nn, dtype=np.float64).astype(np.float32)
+    i = int(np.argmax(f))  # first occurrence of the maximum
+    return i, float(f[i])
+
+
 def pair_dist(x, m, i, j):
     x = _f32(x)
     return lib().or_pair_dist(x, len(x), m, i, j)
@@ -163,13 +212,15 @@ def palmad(x, minL, maxL, iter_cap=200, log_cap=100000):
             [log[i].as_dict() for i in range(min(na, log_cap))])
 
 
-def pd3(x, m, top_k=1, iter_cap=200, log_cap=1000):
-    """Fixed-length discords with the halving schedule; (discords, attempts)."""
+def pd3(x, m, top_k=1, iter_cap=200, log_cap=1000, fast=False):
+    """Fixed-length discords with the halving schedule; (discords, attempts).
+    fast: the vectorised nn profile (for long series)."""
     x = _f32(x)
     sel = (Discord * top_k)()
     log = (Attempt * log_cap)()
     na = C.c_int64(0)
-    ns = lib().or_pd3(x, len(x), m, top_k, iter_cap, sel, log, log_cap, C.byref(na))
+    ns = lib().or_pd3(x, len(x), m, top_k, iter_cap, sel, log, log_cap, C.byref(na),
+                      1 if fast else 0)
     if ns < 0:
         raise RuntimeError("r-schedule exceeded the attempt cap")
     return ([(sel[i].ind, sel[i].dist) for i in range(ns)],

@@ -139,7 +139,12 @@ _SIGS = {
                           C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "paddi_model_predict": ([C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int32,
                              C.c_void_p], C.c_int),
+    "paddi_debug_set": ([C.c_void_p, C.c_int32, C.c_int64], C.c_int),
+    "paddi_debug_get": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int64)], C.c_int),
 }
+
+# test hooks (include/paddi.h, paddi_debug_key)
+DEBUG_FAIL_ALLOC, DEBUG_WAIT_CYCLES, DEBUG_WITHHOLD_STAGE, DEBUG_LAST_PASSES = 1, 2, 3, 4
 
 # Largest n - m + 1 accepted by compute_statistics_noalloc (include/paddi.h).
 NOALLOC_MAX_WINDOWS = 131072
@@ -256,6 +261,17 @@ class Context:
         self._check(lib().paddi_model_predict(self._h, X.ctypes.data, len(X), p.ctypes.data,
                                               1 if bf16 else 0, y.ctypes.data))
         return y
+
+    # ------------------------------------------------------------ test hooks
+    def debug_set(self, key: int, value: int):
+        """Failure injection (DEBUG_*): a failing allocation, a short refine wait
+        limit, a withheld refine pipeline stage."""
+        self._check(lib().paddi_debug_set(self._h, key, int(value)))
+
+    def debug_get(self, key: int) -> int:
+        v = C.c_int64(0)
+        self._check(lib().paddi_debug_get(self._h, key, C.byref(v)))
+        return v.value
 
     def _check(self, s):
         if s != PADDI_OK:

@@ -282,7 +282,7 @@ cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const flo
                                     int32_t *task_counter, int32_t *walked, int32_t num_sms,
                                     cudaStream_t st)
 {
-    if (R < 64 || R > 2048 || (R & 7) || m > P1_MAXM || max_chunks < 1)
+    if (R < 64 || R > 4096 || (R & 7) || m > P1_MAXM || max_chunks < 1)
         return cudaErrorInvalidValue;
     const size_t smem = paddi_phase1_smem(R, m);
     cudaError_t e = paddi_raise_smem_limit((const void *)k_phase1, smem);

@@ -65,7 +65,9 @@ constexpr int UM_KMAX64 = 736;   // largest K' with M = 64
 constexpr int ZSCALE = 8;        // zhat scaled by 2^8 before splitting
 constexpr int WD_ROW = 129;      // float4 entries per shift row of the window data (128 + pad)
 constexpr int WD_BYTES = 8 * WD_ROW * 16;
-constexpr long long UM_WAIT_CYCLES = 4000000000ll; // ~2 s at 1.9 GHz
+// limit of the abort path's drain waits (~2 s at 1.9 GHz): copies and MMAs the
+// kernel issued complete on their own, so these waits end long before it
+constexpr long long kDrainCycles = 4000000000ll;
 constexpr int EPI_WARP0 = 4;     // warps 4..11: epilogue (two per TMEM lane quarter)
 constexpr int EPI_WARPS = 8;
 constexpr int MMA_WARP = 0, LOAD_WARP = 1;
@@ -105,12 +107,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 }
 
 // Bounded wait for the completion of the phase with the given parity;
-// false when the limit was reached.
-__device__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+// false when `limit` clock cycles passed first.
+__device__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit)
 {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > UM_WAIT_CYCLES) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -326,6 +328,9 @@ struct UmShared {
     uint64_t wd_full;      // loader -> epilogue: window data of the tile (or an end token)
     uint64_t wd_empty;     // epilogue -> loader: window data consumed
     uint64_t drain;        // final MMA drain on abort
+    // absolute phase index of the last arrival the loader issued on full_b[s] /
+    // wd_full (-1: none yet); the abort path waits only for those
+    int last_full[2], last_wd;
     uint32_t tmem_base;
     int item, abort, tok;
     volatile int item_dead;
@@ -354,7 +359,8 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
               const int32_t *__restrict__ list, const int32_t *__restrict__ list_count,
               const uint16_t *__restrict__ bq, const float4 *__restrict__ wdq,
               PaddiAttemptDev *att, uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-              int32_t jb, int32_t je, float thr, int32_t grid_ctas)
+              int32_t jb, int32_t je, float thr, int32_t grid_ctas, long long wl,
+              int32_t withhold)
 {
     using X = E16<BF>;
     constexpr int UM_M = MM;
@@ -380,6 +386,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
         mbar_init(&S.wd_empty, EPI_WARPS);
         mbar_init(&S.drain, 1);
         S.abort = 0;
+        S.last_full[0] = S.last_full[1] = S.last_wd = -1;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -450,10 +457,16 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
         // (the build's scratch is stage 1 + the window data)
         if (warp == LOAD_WARP && lane == 0) {
             S.vb[0] = 1;
-            const uint16_t *src = bq + (size_t)blk0 * 2 * cnt;
-            mbar_arrive_expect_tx(&S.full_b[0], (uint32_t)(4 * cnt));
-            bulk_g2s(um_smem + L.b[0][0], src, (uint32_t)(2 * cnt), &S.full_b[0]);
-            bulk_g2s(um_smem + L.b[0][1], src + cnt, (uint32_t)(2 * cnt), &S.full_b[0]);
+            // test hook (withhold != 0): the CTA holding work item 0 never fills
+            // its first stage, so the MMA thread's wait runs out; nothing is in flight
+            const bool skip = withhold && item == 0;
+            if (!skip) {
+                const uint16_t *src = bq + (size_t)blk0 * 2 * cnt;
+                mbar_arrive_expect_tx(&S.full_b[0], (uint32_t)(4 * cnt));
+                bulk_g2s(um_smem + L.b[0][0], src, (uint32_t)(2 * cnt), &S.full_b[0]);
+                bulk_g2s(um_smem + L.b[0][1], src + cnt, (uint32_t)(2 * cnt), &S.full_b[0]);
+                S.last_full[0] = (int)ph.full[0];
+            }
         }
         // ---- candidate operand: 16 x (hi, lo) rows of scaled zhat, then 8 shifted copies
         {
@@ -533,8 +546,9 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             // an end token instead once the item is dead
             auto load_slice = [&](int u) -> bool {
                 const int s = u & 1;
-                if (u >= 2 && !mbar_wait_bounded(&S.mma_done[s], par(ph.done[s] + ((u - 2) >> 1))))
+                if (u >= 2 && !mbar_wait_bounded(&S.mma_done[s], par(ph.done[s] + ((u - 2) >> 1)), wl))
                     return false;
+                S.last_full[s] = (int)(ph.full[s] + (u >> 1));
                 if (S.item_dead) {
                     S.vb[s] = 0;
                     S.tok = u;
@@ -553,10 +567,11 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 if (u + 1 < T) ok = load_slice(u + 1);
                 if (!ok) break;
                 // window data of tile u (after the epilogue is done with tile u-1)
-                if (u >= 1 && !mbar_wait_bounded(&S.wd_empty, par(ph.wde + (u - 1)))) {
+                if (u >= 1 && !mbar_wait_bounded(&S.wd_empty, par(ph.wde + (u - 1)), wl)) {
                     ok = false;
                     break;
                 }
+                S.last_wd = (int)(ph.wdf + u);
                 if (S.tok == u + 1) { // end token: no window data for tile u either
                     S.vw = 0;
                     mbar_arrive(&S.wd_full);
@@ -571,7 +586,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
         } else if (warp == MMA_WARP && lane == 0) {
             for (int u = 0; u < T; ++u) {
                 const int s = u & 1;
-                if (!mbar_wait_bounded(&S.full_b[s], par(ph.full[s] + (u >> 1)))) {
+                if (!mbar_wait_bounded(&S.full_b[s], par(ph.full[s] + (u >> 1)), wl)) {
                     S.abort = 1;
                     break;
                 }
@@ -579,7 +594,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 // end token: its commit completes a phase of mma_done[s] that the
                 // epilogue may still be waiting on for tile u-2
                 if (u >= 2 &&
-                    !mbar_wait_bounded(&S.acc_empty[s], par(ph.acc[s] + ((u - 2) >> 1)))) {
+                    !mbar_wait_bounded(&S.acc_empty[s], par(ph.acc[s] + ((u - 2) >> 1)), wl)) {
                     S.abort = 1;
                     break;
                 }
@@ -612,20 +627,19 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             // the warp is converged and takes the same branch at every tcgen05.ld.
             for (int u = 0; u < T; ++u) {
                 const int s = u & 1;
-                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&S.wd_full, par(ph.wdf + u)))) {
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&S.wd_full, par(ph.wdf + u), wl))) {
                     S.abort = 1;
                     break;
                 }
                 const int vw = __shfl_sync(0xffffffffu, S.vw, 0);
                 if (!__all_sync(0xffffffffu,
-                                mbar_wait_bounded(&S.mma_done[s], par(ph.done[s] + (u >> 1))))) {
+                                mbar_wait_bounded(&S.mma_done[s], par(ph.done[s] + (u >> 1)), wl))) {
                     S.abort = 1;
                     break;
                 }
                 if (!vw) { // end token; its slice twin at tile u+1 is committed too
                     const int s1 = (u + 1) & 1;
-                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&S.mma_done[s1],
-                                                                    par(ph.done[s1] + ((u + 1) >> 1)))))
+                    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&S.mma_done[s1], par(ph.done[s1] + ((u + 1) >> 1)), wl)))
                         S.abort = 1;
                     break;
                 }
@@ -745,15 +759,17 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             atomicExch(&att->status, 3);
             if (mma_issued) { // let the MMAs in flight finish before TMEM goes away
                 umma_commit(&S.drain);
-                mbar_wait_bounded(&S.drain, 0u);
+                mbar_wait_bounded(&S.drain, 0u, kDrainCycles);
             }
         }
         // bulk copies in flight complete on their barriers: wait (bounded) for
-        // the last phase of each before the shared memory goes away
+        // the last phase the loader issued on each before the shared memory goes
+        // away (a phase it never issued is not waited for)
         if (threadIdx.x == 32) {
             for (int s = 0; s < 2; ++s)
-                if (ph.full[s]) mbar_wait_bounded(&S.full_b[s], par(ph.full[s] - 1));
-            if (ph.wdf) mbar_wait_bounded(&S.wd_full, par(ph.wdf - 1));
+                if (S.last_full[s] >= 0)
+                    mbar_wait_bounded(&S.full_b[s], par((uint32_t)S.last_full[s]), kDrainCycles);
+            if (S.last_wd >= 0) mbar_wait_bounded(&S.wd_full, par((uint32_t)S.last_wd), kDrainCycles);
         }
     }
     tc_fence_before();
@@ -806,7 +822,8 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                                      const int32_t *list_count, const uint16_t *bq,
                                      const float4 *wdq, PaddiAttemptDev *att, uint32_t *rho_max,
                                      uint8_t *pruned, int32_t N, int32_t m, int32_t jb, int32_t je,
-                                     float thr_prune, int32_t num_sms, cudaStream_t st)
+                                     float thr_prune, int32_t num_sms, cudaStream_t st,
+                                     long long wait_cycles, int32_t withhold)
 {
     const int kp = kpad_of(m);
     if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
@@ -817,13 +834,15 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
     const size_t smem = L.bytes < 120 * 1024 ? 120 * 1024 : L.bytes;
     void (*kern)(const float *, const float4 *, const float *, const int32_t *, const int32_t *,
                  const int32_t *, const uint16_t *, const float4 *, PaddiAttemptDev *, uint32_t *,
-                 uint8_t *, int32_t, int32_t, int32_t, int32_t, float, int32_t);
+                 uint8_t *, int32_t, int32_t, int32_t, int32_t, float, int32_t, long long,
+                 int32_t);
     if (MM == 128) kern = bf16 ? k_refine_umma<true, 128> : k_refine_umma<false, 128>;
     else kern = bf16 ? k_refine_umma<true, 64> : k_refine_umma<false, 64>;
     cudaError_t e = paddi_raise_smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     const int grid = num_sms;
     kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, bq, wdq, att, rho_max,
-                                         pruned, N, m, jb, je, thr_prune, grid);
+                                         pruned, N, m, jb, je, thr_prune, grid,
+                                         wait_cycles > 0 ? wait_cycles : 4000000000ll, withhold);
     return cudaGetLastError();
 }

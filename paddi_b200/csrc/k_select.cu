@@ -313,7 +313,9 @@ k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
     if (threadIdx.x == 0) {
         const int nr = s_nr;
         att->n_recheck = nr < rc_cap ? nr : rc_cap;
-        if (nr > rc_cap) att->status = 1;
+        // a status set earlier (3: a refine wait ran out) is kept: it explains
+        // an overflow here and must reach the host unchanged
+        if (nr > rc_cap) atomicCAS(&att->status, 0, 1);
         res->n_p1 = C;
         res->n_recheck = nr;
         res->n_cand = certain_c; // completed in k_select

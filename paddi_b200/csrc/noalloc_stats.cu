@@ -17,7 +17,10 @@
 // Rules a caller must follow:
 //   * the first call on a device resolves the array's device address with
 //     cudaGetSymbolAddress; make that first call before any stream capture
-//     begins on the device;
+//     begins on the device.  Every later call that is not being captured
+//     resolves it again (a host-side lookup), so the address stays right after
+//     cudaDeviceReset or under another context of the same device; a call
+//     under capture uses the address of the device's last uncaptured call;
 //   * every call on a device uses the same array, so calls whose GPU work can
 //     overlap (other streams, other host threads) race with each other: keep
 //     them on one stream, one after another;
@@ -68,10 +71,20 @@ PADDI_API paddi_status paddi_compute_statistics_noalloc(const float *d_T, float 
         return PADDI_ERR_NO_DEVICE;
     }
     if (dev < 0 || dev >= kMaxDevices) return PADDI_ERR_INVALID_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // under stream capture the lookup is not repeated (nor is anything but the
+    // two kernels and the memset enqueued); otherwise it is, so a module that
+    // was loaded again (device reset, another context) is found at its new address
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        cap = cudaStreamCaptureStatusActive; // unknown: treat as captured
+    }
     unsigned char *base = nullptr;
     {
         std::lock_guard<std::mutex> g(g_lock);
-        if (!g_base[dev]) { // set-up, once per device, with that device current
+        if (!g_base[dev] || cap == cudaStreamCaptureStatusNone) {
+            // set-up with this device current: the scratch's device address
             void *p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_stats_scratch);
             if (e != cudaSuccess || !p) {
@@ -82,7 +95,6 @@ PADDI_API paddi_status paddi_compute_statistics_noalloc(const float *d_T, float 
         }
         base = g_base[dev];
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     int32_t *count = reinterpret_cast<int32_t *>(base + kOffCount);
     double *mu64 = reinterpret_cast<double *>(base + kOffMu64);
     double *inv64 = reinterpret_cast<double *>(base + kOffInv64);

@@ -96,6 +96,12 @@ struct paddi_ctx {
     int32_t *d_flatcount = nullptr;
     PaddiAttemptResult *h_res = nullptr;
     bool umma_ok = false;
+    // test hooks (paddi_debug_set): fail the k-th next device allocation; the
+    // refine's barrier-wait limit; withhold one refine pipeline stage
+    int64_t fail_alloc = 0;
+    long long wait_cycles = 0;
+    int32_t withhold = 0;
+    int32_t last_passes = 0; // selection passes of the last attempt
 };
 
 namespace {
@@ -123,6 +129,16 @@ paddi_status fail(paddi_ctx *c, paddi_status s, const std::string &msg)
                                                              : PADDI_ERR_CUDA,              \
                         std::string(#call) + ": " + cudaGetErrorString(e_));                \
     } while (0)
+
+// Every device allocation of a context goes through here, so a test can make
+// one fail (PADDI_DEBUG_FAIL_ALLOC) and check that PADDI_ERR_OUT_OF_MEMORY
+// reaches the caller.
+template <typename T>
+cudaError_t dmalloc(paddi_ctx *ctx, T **p, size_t bytes)
+{
+    if (ctx->fail_alloc > 0 && --ctx->fail_alloc == 0) return cudaErrorMemoryAllocation;
+    return cudaMalloc((void **)p, bytes);
+}
 
 template <typename T>
 void dfree(T *&p)
@@ -165,26 +181,26 @@ paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
     CK(cudaStreamSynchronize(ctx->st));
     free_buffers(ctx);
     const size_t W = n + PADDI_PAD_WIN + 64; // windows (upper bound) incl. the zeroed tail
-    CK(cudaMalloc(&ctx->d_x, sizeof(float) * (n + 64)));
-    CK(cudaMalloc(&ctx->d_wst, sizeof(float4) * W));
-    CK(cudaMalloc(&ctx->d_mu, sizeof(float) * W));
-    CK(cudaMalloc(&ctx->d_mu64, sizeof(double) * W));
-    CK(cudaMalloc(&ctx->d_inv64, sizeof(double) * W));
-    CK(cudaMalloc(&ctx->d_flat, W));
-    CK(cudaMalloc(&ctx->d_alive, W));
-    CK(cudaMalloc(&ctx->d_pruned, W));
-    CK(cudaMalloc(&ctx->d_cand, sizeof(int32_t) * W));
-    CK(cudaMalloc(&ctx->d_rcslot, sizeof(int32_t) * W));
-    CK(cudaMalloc(&ctx->d_rho, sizeof(uint32_t) * W));
-    CK(cudaMalloc(&ctx->d_list[0], sizeof(int32_t) * W));
-    CK(cudaMalloc(&ctx->d_list[1], sizeof(int32_t) * W));
+    CK(dmalloc(ctx, &ctx->d_x, sizeof(float) * (n + 64)));
+    CK(dmalloc(ctx, &ctx->d_wst, sizeof(float4) * W));
+    CK(dmalloc(ctx, &ctx->d_mu, sizeof(float) * W));
+    CK(dmalloc(ctx, &ctx->d_mu64, sizeof(double) * W));
+    CK(dmalloc(ctx, &ctx->d_inv64, sizeof(double) * W));
+    CK(dmalloc(ctx, &ctx->d_flat, W));
+    CK(dmalloc(ctx, &ctx->d_alive, W));
+    CK(dmalloc(ctx, &ctx->d_pruned, W));
+    CK(dmalloc(ctx, &ctx->d_cand, sizeof(int32_t) * W));
+    CK(dmalloc(ctx, &ctx->d_rcslot, sizeof(int32_t) * W));
+    CK(dmalloc(ctx, &ctx->d_rho, sizeof(uint32_t) * W));
+    CK(dmalloc(ctx, &ctx->d_list[0], sizeof(int32_t) * W));
+    CK(dmalloc(ctx, &ctx->d_list[1], sizeof(int32_t) * W));
     if (ctx->umma_ok) {
         const int64_t blocks = paddi_tile_blocks((int64_t)n);
-        CK(cudaMalloc(&ctx->d_bq, sizeof(uint16_t) * (size_t)(blocks * paddi_tile_block_elems_max())));
-        CK(cudaMalloc(&ctx->d_wdq, sizeof(float4) * (size_t)(blocks * paddi_tile_wd_entries())));
+        CK(dmalloc(ctx, &ctx->d_bq, sizeof(uint16_t) * (size_t)(blocks * paddi_tile_block_elems_max())));
+        CK(dmalloc(ctx, &ctx->d_wdq, sizeof(float4) * (size_t)(blocks * paddi_tile_wd_entries())));
     }
-    CK(cudaMalloc(&ctx->d_recheck, sizeof(int32_t) * PADDI_MAX_RECHECK));
-    CK(cudaMalloc(&ctx->d_nn64, sizeof(unsigned long long) * PADDI_MAX_RECHECK));
+    CK(dmalloc(ctx, &ctx->d_recheck, sizeof(int32_t) * PADDI_MAX_RECHECK));
+    CK(dmalloc(ctx, &ctx->d_nn64, sizeof(unsigned long long) * PADDI_MAX_RECHECK));
     ctx->rc_cap = PADDI_MAX_RECHECK;
     CK(cudaMemsetAsync(ctx->d_wst, 0, sizeof(float4) * W, ctx->st));
     CK(cudaMemsetAsync(ctx->d_mu, 0, sizeof(float) * W, ctx->st));
@@ -251,11 +267,11 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     const float guard = guard_of(ctx, kernel);
     const float thr = (float)(1.0 - (double)r2 / (2.0 * (double)m));
     const float thr_prune = thr + guard;
+    // phase-1 rows per task (the reference's SEGMENT_N); validated at the ABI
+    // (segment_len_ok), rounded up to a multiple of 8 rows
     int R = (int)ctx->opts.segment_len;
     if (R <= 0) R = 256;
     R = (R + 7) & ~7;
-    if (R < 64) R = 64;
-    if (R > 1024) R = 1024;
     const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 12;
     cudaStream_t st = ctx->st;
     CK(cudaEventRecord(ctx->ev[0], st));
@@ -300,7 +316,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
                                         ctx->d_cand, ctx->d_list[a],
                                         &ctx->d_att->list_count[a], ctx->d_bq, ctx->d_wdq,
                                         ctx->d_att, ctx->d_rho, ctx->d_pruned, N, m, jb, je,
-                                        thr_prune, ctx->num_sms, st));
+                                        thr_prune, ctx->num_sms, st, ctx->wait_cycles,
+                                        ctx->withhold));
         else
             CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
                                         &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,
@@ -346,14 +363,18 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
             spec = true;
         }
         CK(cudaStreamSynchronize(st));
+        ctx->last_passes = pass + 1;
+        if (ctx->h_res->status == 3) // a refine wait ran out: no redo can help
+            return fail(ctx, PADDI_ERR_CUDA, "tensor-core refine: a barrier wait timed out (m=" +
+                                                 std::to_string(m) + ")");
         if (ctx->h_res->status == 1) {
             // more windows need the exact value than the queue holds: grow it and redo
             int32_t cap = ctx->rc_cap;
             while (cap < ctx->h_res->n_recheck) cap *= 2;
             dfree(ctx->d_recheck);
             dfree(ctx->d_nn64);
-            CK(cudaMalloc(&ctx->d_recheck, sizeof(int32_t) * (size_t)cap));
-            CK(cudaMalloc(&ctx->d_nn64, sizeof(unsigned long long) * (size_t)cap));
+            CK(dmalloc(ctx, &ctx->d_recheck, sizeof(int32_t) * (size_t)cap));
+            CK(dmalloc(ctx, &ctx->d_nn64, sizeof(unsigned long long) * (size_t)cap));
             ctx->rc_cap = cap;
         } else if (ctx->h_res->status == 2) {
             // a pick had no exact value: queue everything up to the cut and redo
@@ -369,8 +390,6 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         CK(cudaMemsetAsync(&ctx->d_att->recheck_next, 0, sizeof(int32_t), st));
         CK(cudaMemsetAsync(&ctx->d_att->status, 0, sizeof(int32_t), st));
     }
-    if (ctx->h_res->status == 3)
-        return fail(ctx, PADDI_ERR_CUDA, "tensor-core refine: a barrier wait timed out");
     if (ctx->h_res->status == 1)
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT,
                     "more windows than the FP64 recheck capacity fall inside the guard band (m=" +
@@ -434,6 +453,11 @@ void fill_log(paddi_attempt_log *L, int m, float r, float r2, int top_k, const A
     L->r_source = 0;
     L->ms_guide = 0.f;
 }
+
+// Phase-1 segment lengths this build runs: 0 (default 256) or 64..4096 rows.
+// The reference caps SEGMENT_N at its 1024-thread block (src/PD3.cuh:20); here
+// a segment is a task of one warp, so longer segments only cost occupancy.
+bool segment_len_ok(uint32_t seg) { return seg == 0 || (seg >= 64 && seg <= 4096); }
 
 bool valid_lengths(size_t n, uint32_t minL, uint32_t maxL)
 {
@@ -588,8 +612,8 @@ paddi_status attempt_profile(paddi_ctx *ctx, int m, int32_t N, float r2, std::ve
 {
     if (!ctx->d_pc) {
         const size_t W = ctx->cap_n + PADDI_PAD_WIN + 64;
-        CK(cudaMalloc(&ctx->d_pc, sizeof(int32_t) * W));
-        CK(cudaMalloc(&ctx->d_pn, sizeof(float) * W));
+        CK(dmalloc(ctx, &ctx->d_pc, sizeof(int32_t) * W));
+        CK(dmalloc(ctx, &ctx->d_pn, sizeof(float) * W));
     }
     CK(paddi_launch_scatter(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned, ctx->d_rcslot,
                             ctx->d_nn64, ctx->d_flat, N, m, r2, ctx->d_pc, ctx->d_pn, ctx->st));
@@ -627,7 +651,7 @@ paddi_status palmad_impl(paddi_ctx *ctx, const float *x, size_t n, uint32_t minL
         if (ctx->G_cap < W) {
             dfree(ctx->d_G);
             ctx->G_cap = 0;
-            CK(cudaMalloc(&ctx->d_G, sizeof(double) * 2 * W)); // two buffers
+            CK(dmalloc(ctx, &ctx->d_G, sizeof(double) * 2 * W)); // two buffers
             ctx->G_cap = W;
         }
         // the dot products of an earlier call belong to another series
@@ -809,6 +833,10 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
             return PADDI_ERR_INVALID_ARG;
         }
         ctx->opts = *opts;
+        if (!segment_len_ok(ctx->opts.segment_len)) {
+            delete ctx;
+            return PADDI_ERR_UNSUPPORTED;
+        }
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= ctx->opts.device ||
@@ -966,6 +994,9 @@ PADDI_API paddi_status paddi_pd3(paddi_ctx *ctx, const float *series, size_t n, 
     if (!series || !out || !n_out || top_k < 1 || top_k > PADDI_MAX_TOPK ||
         !valid_lengths(n, m, m))
         return fail(ctx, PADDI_ERR_INVALID_ARG, "invalid series, length, top_k or output");
+    if (!segment_len_ok(segment_len))
+        return fail(ctx, PADDI_ERR_UNSUPPORTED,
+                    "segment_len " + std::to_string(segment_len) + " outside 64..4096");
     *n_out = 0;
     if (n_log) *n_log = 0;
     CK(cudaSetDevice(ctx->device));
@@ -1073,6 +1104,41 @@ PADDI_API paddi_status paddi_do_pd3(paddi_ctx *ctx, const float *d_T, size_t n, 
     return PADDI_OK;
 }
 
+// ================================================================ test hooks
+PADDI_API paddi_status paddi_debug_set(paddi_ctx *ctx, int32_t key, int64_t value)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    switch (key) {
+    case PADDI_DEBUG_FAIL_ALLOC:
+        if (value < 0) break;
+        ctx->fail_alloc = value;
+        return PADDI_OK;
+    case PADDI_DEBUG_WAIT_CYCLES:
+        if (value < 0) break;
+        ctx->wait_cycles = (long long)value;
+        return PADDI_OK;
+    case PADDI_DEBUG_WITHHOLD_STAGE:
+        ctx->withhold = value != 0;
+        return PADDI_OK;
+    default:
+        break;
+    }
+    return fail(ctx, PADDI_ERR_INVALID_ARG, "paddi_debug_set: unknown key or bad value");
+}
+
+PADDI_API paddi_status paddi_debug_get(paddi_ctx *ctx, int32_t key, int64_t *value)
+{
+    if (!ctx || !value) return PADDI_ERR_INVALID_ARG;
+    switch (key) {
+    case PADDI_DEBUG_FAIL_ALLOC: *value = ctx->fail_alloc; return PADDI_OK;
+    case PADDI_DEBUG_WAIT_CYCLES: *value = ctx->wait_cycles; return PADDI_OK;
+    case PADDI_DEBUG_WITHHOLD_STAGE: *value = ctx->withhold; return PADDI_OK;
+    case PADDI_DEBUG_LAST_PASSES: *value = ctx->last_passes; return PADDI_OK;
+    default: break;
+    }
+    return fail(ctx, PADDI_ERR_INVALID_ARG, "paddi_debug_get: unknown key");
+}
+
 // ============================================================ learned r model
 PADDI_API paddi_status paddi_r_features(const paddi_discord *out, uint32_t j, uint32_t minL,
                                         float lb, float flat_frac, uint32_t prev_attempts,
@@ -1118,11 +1184,11 @@ PADDI_API paddi_status paddi_model_grad(paddi_ctx *ctx, const float *X, const fl
         return fail(ctx, PADDI_ERR_INVALID_ARG, "model_grad: null argument or empty data");
     CK(cudaSetDevice(ctx->device));
     DevBuf dX, dY, dP, dG, dL;
-    CK(cudaMalloc(&dX.p, sizeof(float) * MLP_NFEAT * n));
-    CK(cudaMalloc(&dY.p, sizeof(float) * n));
-    CK(cudaMalloc(&dP.p, sizeof(float) * MLP_NPARAM));
-    CK(cudaMalloc(&dG.p, sizeof(float) * MLP_NPARAM));
-    CK(cudaMalloc(&dL.p, sizeof(float)));
+    CK(dmalloc(ctx, &dX.p, sizeof(float) * MLP_NFEAT * n));
+    CK(dmalloc(ctx, &dY.p, sizeof(float) * n));
+    CK(dmalloc(ctx, &dP.p, sizeof(float) * MLP_NPARAM));
+    CK(dmalloc(ctx, &dG.p, sizeof(float) * MLP_NPARAM));
+    CK(dmalloc(ctx, &dL.p, sizeof(float)));
     cudaStream_t st = ctx->st;
     CK(cudaMemcpyAsync(dX.p, X, sizeof(float) * MLP_NFEAT * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dY.p, Y, sizeof(float) * n, cudaMemcpyHostToDevice, st));
@@ -1146,10 +1212,10 @@ PADDI_API paddi_status paddi_model_predict(paddi_ctx *ctx, const float *X, uint3
     CK(cudaSetDevice(ctx->device));
     DevBuf dX, dY, dP, dQ;
     cudaStream_t st = ctx->st;
-    CK(cudaMalloc(&dX.p, sizeof(float) * MLP_NFEAT * n));
-    CK(cudaMalloc(&dY.p, sizeof(float) * n));
-    CK(cudaMalloc(&dP.p, sizeof(float) * MLP_NPARAM));
-    CK(cudaMalloc(&dQ.p, 2 * MLP_NPARAM));
+    CK(dmalloc(ctx, &dX.p, sizeof(float) * MLP_NFEAT * n));
+    CK(dmalloc(ctx, &dY.p, sizeof(float) * n));
+    CK(dmalloc(ctx, &dP.p, sizeof(float) * MLP_NPARAM));
+    CK(dmalloc(ctx, &dQ.p, 2 * MLP_NPARAM));
     CK(cudaMemcpyAsync(dX.p, X, sizeof(float) * MLP_NFEAT * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dP.p, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, st));
     if (bf16) {
@@ -1173,13 +1239,13 @@ PADDI_API paddi_status paddi_model_train(paddi_ctx *ctx, const float *X, const f
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->st;
     DevBuf dX, dY, dP, dG, dM, dV, dL;
-    CK(cudaMalloc(&dX.p, sizeof(float) * MLP_NFEAT * n));
-    CK(cudaMalloc(&dY.p, sizeof(float) * n));
-    CK(cudaMalloc(&dP.p, sizeof(float) * MLP_NPARAM));
-    CK(cudaMalloc(&dG.p, sizeof(float) * MLP_NPARAM));
-    CK(cudaMalloc(&dM.p, sizeof(float) * MLP_NPARAM));
-    CK(cudaMalloc(&dV.p, sizeof(float) * MLP_NPARAM));
-    CK(cudaMalloc(&dL.p, sizeof(float) * (epochs ? epochs : 1)));
+    CK(dmalloc(ctx, &dX.p, sizeof(float) * MLP_NFEAT * n));
+    CK(dmalloc(ctx, &dY.p, sizeof(float) * n));
+    CK(dmalloc(ctx, &dP.p, sizeof(float) * MLP_NPARAM));
+    CK(dmalloc(ctx, &dG.p, sizeof(float) * MLP_NPARAM));
+    CK(dmalloc(ctx, &dM.p, sizeof(float) * MLP_NPARAM));
+    CK(dmalloc(ctx, &dV.p, sizeof(float) * MLP_NPARAM));
+    CK(dmalloc(ctx, &dL.p, sizeof(float) * (epochs ? epochs : 1)));
     CK(cudaMemcpyAsync(dP.p, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(dG.p, 0, sizeof(float) * MLP_NPARAM, st));
     CK(cudaMemsetAsync(dM.p, 0, sizeof(float) * MLP_NPARAM, st));

@@ -124,13 +124,17 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
 
 // Tensor-core refine over windows [jb, je) (jb a multiple of the tile width,
 // je too or je = N).  bq / wdq: the per-length tile data of
-// paddi_launch_tile_prep.
+// paddi_launch_tile_prep.  wait_cycles: limit of every barrier wait (<= 0:
+// about 2 s); a wait that runs out sets att->status = 3 and the kernel
+// returns.  withhold != 0 is a test hook: the CTA holding work item 0 never
+// fills that item's first stage, so its waits run out.
 cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *wst,
                                      const float *mu, const int32_t *cand, const int32_t *list,
                                      const int32_t *list_count, const uint16_t *bq,
                                      const float4 *wdq, PaddiAttemptDev *att, uint32_t *rho_max,
                                      uint8_t *pruned, int32_t N, int32_t m, int32_t jb, int32_t je,
-                                     float thr_prune, int32_t num_sms, cudaStream_t st);
+                                     float thr_prune, int32_t num_sms, cudaStream_t st,
+                                     long long wait_cycles = 0, int32_t withhold = 0);
 
 // Per-length tile data of the tensor-core refine: for every block of
 // paddi_tile_width() windows, the split 16-bit series slice (bq, at most

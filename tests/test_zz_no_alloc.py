@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import paddi_b200 as P
+from oracle import oracle as O
 from paddi_b200 import datagen
 
 pytestmark = pytest.mark.gpu
@@ -50,6 +51,10 @@ def test_noalloc_statistics_match_the_context_entry_point_twice():
             got_mean, got_std = _stats_noalloc(dT, n, m)
             np.testing.assert_allclose(got_mean, want_mean, rtol=RTOL, atol=ATOL)
             np.testing.assert_allclose(got_std, want_std, rtol=RTOL, atol=ATOL)
+            # and independently of the CUDA kernels: the FP64 oracle's statistics
+            mu, sd, _ = O.window_stats(x[:n], m)
+            np.testing.assert_allclose(got_mean, mu, rtol=RTOL, atol=ATOL)
+            np.testing.assert_allclose(got_std, sd, rtol=2e-6, atol=ATOL)
 
 
 def test_noalloc_statistics_refuse_inputs_beyond_the_limit():
