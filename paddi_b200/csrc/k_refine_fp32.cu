@@ -92,7 +92,7 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
             cw[threadIdx.x] = w;
             cp[threadIdx.x] = pos;
             dead[threadIdx.x] = !v || __ldcg(pruned + pos);
-            cf[threadIdx.x] = v ? wst[w].w : 0.f;
+            cf[threadIdx.x] = (v && wst[w].z == 0.f) ? 1.f : 0.f; // flat candidate
         }
         __syncthreads();
         int alive = 0;
@@ -126,7 +126,7 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
             for (int q = threadIdx.x; q < RF_TW; q += RF_THREADS) {
                 const float4 ws = wst[j0 + q]; // zero beyond N
                 S.cinv[q] = ws.z;
-                S.cflt[q] = ws.w;
+                S.cflt[q] = ws.z == 0.f ? 1.f : 0.f; // flat window (or the padded tail)
                 S.cmu[q] = mu[j0 + q];
             }
             __syncthreads();

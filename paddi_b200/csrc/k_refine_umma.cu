@@ -434,7 +434,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             S.cw[threadIdx.x] = w;
             S.cp[threadIdx.x] = pos;
             S.dead[threadIdx.x] = !v || __ldcg(pruned + pos);
-            S.cflat[threadIdx.x] = v ? wst[w].w : 0.f;
+            S.cflat[threadIdx.x] = (v && wst[w].z == 0.f) ? 1.f : 0.f; // flat candidate
             S.rmax[threadIdx.x] = f2ord(-INFINITY);
         }
         if (threadIdx.x == 0) {

@@ -134,7 +134,7 @@ k_window_stats(const float *__restrict__ x, int64_t n, int32_t m, int32_t N, flo
             df = (float)((xe - xb) * 0.5);
             dg = (float)((xe - mu_n) + (xb - mu_i));
         }
-        wst[i] = make_float4(df, dg, (float)iv, fl ? 1.f : 0.f);
+        wst[i] = make_float4(df, dg, (float)iv, fl ? 0.f : (float)nrm);
         mu[i] = (float)mu_i;
         mu64[i] = mu_i;
         inv64[i] = iv;

@@ -278,8 +278,9 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     CK(cudaMemsetAsync(ctx->d_alive, 1, (size_t)N, st));
     CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
     int launches = 0;
-    CK(paddi_launch_phase1_dev(x, ctx->d_wst, ctx->d_mu, ctx->d_alive, N, m, R, chunks, thr_prune,
-                               &ctx->d_att->task_next, &ctx->d_att->p1_walked, ctx->num_sms, st));
+    CK(paddi_launch_phase1_dev(x, ctx->d_wst, ctx->d_mu, ctx->d_mu64, ctx->d_alive, N, m, R,
+                               chunks, thr, &ctx->d_att->task_next, &ctx->d_att->p1_walked,
+                               ctx->num_sms, st));
     ++launches;
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(paddi_launch_compact(ctx->d_alive, N, ctx->d_cand, ctx->d_rho, ctx->d_pruned,

@@ -4,9 +4,10 @@
 // Per-window data for one subsequence length m, laid out in HBM as arrays
 // over the N = n - m + 1 windows (plus PADDI_PAD_WIN zeroed entries so tiles
 // may read past the end without bounds checks):
-//   wst[i]  float4 {df_i, dg_i, inv_i, flat_i}   -- diagonal-update terms
+//   wst[i]  float4 {df_i, dg_i, inv_i, n_i}   -- diagonal-update terms
 //           df_i = (x[i+m] - x[i]) / 2,  dg_i = (x[i+m] - mu_{i+1}) + (x[i] - mu_i)
-//           inv_i = 1 / |x_i - mu_i| (0 for a flat window), flat_i in {0, 1}
+//           n_i = |x_i - mu_i| (the window's norm), inv_i = 1 / n_i; both 0 for
+//           a flat window (window i is flat iff inv_i == 0)
 //   mu[i]   float  window mean
 //   mu64[i], inv64[i]  FP64 mean and inverse norm (recheck path)
 //   flat[i] uint8
@@ -17,7 +18,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#define PADDI_PAD_WIN 4096 /* zeroed tail entries after the last window */
+/* zeroed tail entries after the last window: covers the columns a phase-1
+ * task of up to 4096 rows reads past the end (rows + 256) and a tile of the
+ * tensor-core refine (2048 windows) */
+#define PADDI_PAD_WIN 4608
 
 namespace paddi {
 
@@ -99,9 +103,11 @@ cudaError_t paddi_launch_stats(const float *x, int64_t n, int32_t m, float4 *wst
 // flat_span (optional): two zeroed ints that receive {INT_MAX - lowest flat
 // window, highest flat window + 1} (both stay 0 without flat windows).
 
+// Phase 1 at threshold thr = 1 - r^2 / (2m): an exact test (the kernel bounds
+// its own FP32 rounding, no guard band).
 cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const float *mu,
-                                    uint8_t *alive, int32_t N, int32_t m, int32_t R,
-                                    int32_t max_chunks, float thr_prune,
+                                    const double *mu64, uint8_t *alive, int32_t N, int32_t m,
+                                    int32_t R, int32_t max_chunks, float thr,
                                     int32_t *task_counter, int32_t *walked, int32_t num_sms,
                                     cudaStream_t st);
 
