@@ -347,9 +347,15 @@ def run_paddi(args, world, rank, local):
     f32 = [e for e in last if e["refine_kernel"] == 1]
 
     def rate(es):
-        ms = sum(e["ms_refine"] for e in es)
+        # the refine launches alone (the rounds' candidate re-compaction excluded)
+        ms = sum(e["ms_refine_kernel"] for e in es)
         fl = sum(2.0 * e["m"] * e["refine_pairs"] for e in es)
         return (fl / (ms / 1e3) / 1e12 if ms > 0 else 0.0), ms
+
+    def live_rate(es):
+        ms = sum(e["ms_refine_kernel"] for e in es)
+        fl = sum(2.0 * e["m"] * e["refine_live_pairs"] for e in es)
+        return fl / (ms / 1e3) / 1e12 if ms > 0 else 0.0
 
     if tc:
         achieved, ms_tc = rate(tc)
@@ -359,7 +365,10 @@ def run_paddi(args, world, rank, local):
                 "traffic_launch": REFINE_TRAFFIC_LAUNCH, "kernel": "k_refine_umma",
                 "peak_source": f"bf16 dense {src} {bf16} TFLOP/s / 3 (split operands issue 3 MMAs)",
                 "work": "2*m FLOP per (candidate, window) pair evaluated",
-                "kernel_ms_per_step": ms_tc, "attempts": len(tc)}
+                "kernel_ms_per_step": ms_tc, "attempts": len(tc),
+                "live_pairs_achieved": live_rate(tc),
+                "live_pairs_note": "pairs whose candidate was still unpruned when its tile "
+                                   "started (the rest are dead rows of a 16-candidate tile)"}
     else:
         achieved, ms32 = rate(f32)
         peak = 148 * 128 * 2 * 1.965e9 / 1e12  # FP32 FMA, nominal
@@ -369,6 +378,22 @@ def run_paddi(args, world, rank, local):
                 "work": "2*m FLOP per (candidate, window) pair evaluated",
                 "kernel_ms_per_step": ms32, "attempts": len(f32)}
     roof["phase_ms"] = tot
+    # phase 1 (diagonal-strip candidate selection on CUDA cores): 8 FLOP per
+    # (row, diagonal) pair walked (two covariance-update FMAs, the pair test,
+    # counted as in the reference's distance formula), over the phase-1 time
+    # (the kernel plus a 2 MB flag reset), against the nominal FP32 peak at the
+    # clock sampled during the run
+    p1_pairs = sum(e["p1_pairs"] for e in last)
+    p1_ms = tot["ms_phase1"]
+    mhz = (clocks.get("sm_mhz") or 1965.0)
+    p1_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    p1_ach = 8.0 * p1_pairs / (p1_ms / 1e3) / 1e12 if p1_ms > 0 else 0.0
+    roof["phase1"] = {"bound": "fp32", "achieved": p1_ach, "peak": p1_peak, "unit": "TFLOP/s",
+                      "frac": p1_ach / p1_peak, "kernel": "k_phase1",
+                      "peak_source": f"nominal FP32 FMA peak, 148 SMs x 128 lanes x 2 at {mhz:.0f} "
+                                     "MHz (no measured FP32 figure)",
+                      "work": "8 FLOP per (row, diagonal) pair walked",
+                      "pairs_per_step": p1_pairs, "kernel_ms_per_step": p1_ms}
     if tc and f32:
         a32, ms32 = rate(f32)
         roof["fp32_part"] = {"achieved": a32, "ms_per_step": ms32, "attempts": len(f32)}

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PADDI_ABI_VERSION 1
+#define PADDI_ABI_VERSION 2
 
 typedef enum paddi_status {
     PADDI_OK = 0,
@@ -113,6 +113,13 @@ typedef struct paddi_attempt_log {
     float lb;             /* exact nn at this length of the previous length's top-1 window
                              (a lower bound on this length's top-1 distance); 0 if not computed */
     float flat_frac;      /* fraction of flat windows at this length */
+    int64_t p1_pairs;     /* (row, diagonal) pairs phase 1 walked */
+    int64_t refine_live_pairs; /* of refine_pairs, those whose candidate was still
+                                  unpruned when its tile started */
+    float ms_refine_kernel; /* the refine launches alone (ms_refine less the rounds'
+                               candidate re-compaction) */
+    int32_t n_fragile;    /* windows whose rounding bound in the refine exceeds the
+                             guard band; their pairs were evaluated in FP64 */
 } paddi_attempt_log;
 
 typedef struct paddi_ctx paddi_ctx;

@@ -72,7 +72,9 @@ class _Log(C.Structure):
                 ("ms_phase1", C.c_float), ("ms_refine", C.c_float), ("ms_select", C.c_float),
                 ("ms_total", C.c_float), ("refine_pairs", C.c_int64), ("n_launches", C.c_int32),
                 ("refine_kernel", C.c_int32), ("r_source", C.c_int32), ("ms_guide", C.c_float),
-                ("lb", C.c_float), ("flat_frac", C.c_float)]
+                ("lb", C.c_float), ("flat_frac", C.c_float), ("p1_pairs", C.c_int64),
+                ("refine_live_pairs", C.c_int64), ("ms_refine_kernel", C.c_float),
+                ("n_fragile", C.c_int32)]
 
     def as_dict(self):
         return {"m": self.m, "r": self.r, "r2": self.r2, "found": self.found,
@@ -83,7 +85,9 @@ class _Log(C.Structure):
                 "ms_total": self.ms_total, "refine_pairs": self.refine_pairs,
                 "n_launches": self.n_launches, "refine_kernel": self.refine_kernel,
                 "r_source": self.r_source, "ms_guide": self.ms_guide, "lb": self.lb,
-                "flat_frac": self.flat_frac}
+                "flat_frac": self.flat_frac, "p1_pairs": self.p1_pairs,
+                "refine_live_pairs": self.refine_live_pairs,
+                "ms_refine_kernel": self.ms_refine_kernel, "n_fragile": self.n_fragile}
 
 
 @dataclass(frozen=True)

@@ -18,12 +18,23 @@
 //   * the epilogue forms rho = <z_c, x_j - mu_j> inv_j, applies the
 //     trivial-match exclusion |c - j| >= m-1, keeps the running maximum
 //     (maximum rho == minimum distance) and flags a candidate as pruned as
-//     soon as rho > thr_prune (early abandoning: an item stops when all 32 of
-//     its candidates are pruned, and later items of a fully pruned tile are
-//     skipped);
+//     soon as its correlation with some window exceeds thr (early abandoning:
+//     an item stops when all 32 of its candidates are pruned, and later items
+//     of a fully pruned tile are skipped);
 //   * one atomicMax per candidate per item on an order-preserving integer
 //     image of rho (no CAS loop).
+// Rounding: the dot products are summed in two levels (blocks of 64 terms),
+// so a correlation with window j is within g_j = window_bound(E, A_j) of the
+// exact one, A_j the amplification |x_j - sh| / |x_j - mu_j| of the chunk's
+// shift.  Windows with g_j above gcap are fragile: their inverse norm is
+// replaced by NaN (every maximum skips them) and they are evaluated in FP64
+// by the fragile pass.  The chunk's largest other g_j, G, is subtracted from
+// its correlations for the prune test and added back to the kept maxima, so
+// they are the middle of an interval of half-width at most gcap.  Chunks start
+// at multiples of 256 windows, so the fragile set depends only on the length.
 #include <float.h>
+
+#include <cmath>
 
 #include "paddi_internal.cuh"
 
@@ -46,12 +57,14 @@ struct RfSmem {
     float *cflt;  // [RF_TW]
 };
 
+constexpr int RF_SUMBLK = 64; // two-level sums: terms per partial sum
+
 __global__ void __launch_bounds__(RF_THREADS)
 k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
               const float *__restrict__ mu, const int32_t *__restrict__ cand,
               const int32_t *__restrict__ list, const int32_t *__restrict__ list_count,
               PaddiAttemptDev *att, uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-              int32_t jb, int32_t je, float thr, int32_t grid_ctas)
+              int32_t jb, int32_t je, float thr, int32_t grid_ctas, float E, float gcap)
 {
     extern __shared__ __align__(16) unsigned char rf_smem[];
     const int mpad = (m + 7) & ~7;
@@ -62,6 +75,7 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
     S.cmu = S.cinv + RF_TW;
     S.cflt = S.cmu + RF_TW;
     __shared__ int s_item, s_alive;
+    __shared__ float s_gred[RF_THREADS / 32];
     __shared__ int cw[RF_TC], cp[RF_TC];
     __shared__ float cf[RF_TC], zsum[RF_TC];
     __shared__ uint8_t dead[RF_TC];
@@ -109,9 +123,13 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
             S.zT[e] = z;
         }
         __syncthreads();
-        if (threadIdx.x < RF_TC) {
+        if (threadIdx.x < RF_TC) { // two-level sum of the candidate's z
             float s = 0.f;
-            for (int k = 0; k < m; ++k) s += S.zT[k * RF_TC + threadIdx.x];
+            for (int k0 = 0; k0 < m; k0 += RF_SUMBLK) {
+                float p = 0.f;
+                for (int k = k0; k < min(m, k0 + RF_SUMBLK); ++k) p += S.zT[k * RF_TC + threadIdx.x];
+                s += p;
+            }
             zsum[threadIdx.x] = s;
         }
         const int j_lo = jb + split * span, j_hi = min(je, j_lo + span);
@@ -123,18 +141,29 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
                 const int g = j0 + p;
                 S.xs[xpad(p)] = (g < N + m - 1 ? x[g] : sh) - sh;
             }
+            float gq = 0.f; // the chunk's largest bound over its non-fragile windows
             for (int q = threadIdx.x; q < RF_TW; q += RF_THREADS) {
                 const float4 ws = wst[j0 + q]; // zero beyond N
-                S.cinv[q] = ws.z;
+                const float mq = mu[j0 + q];
+                const float g = paddi::window_bound(ws.z, mq, sh, (float)m, E, 0.f);
+                const bool frag = j0 + q < N && g > gcap;
+                if (!frag) gq = fmaxf(gq, g);
+                S.cinv[q] = frag ? __int_as_float(0x7fffffff) : ws.z;
                 S.cflt[q] = ws.z == 0.f ? 1.f : 0.f; // flat window (or the padded tail)
-                S.cmu[q] = mu[j0 + q];
+                S.cmu[q] = mq;
             }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) gq = fmaxf(gq, __shfl_xor_sync(0xffffffffu, gq, o));
+            if (lane == 0) s_gred[warp] = gq;
             __syncthreads();
-            float acc[4][8];
+            float G = 0.f;
+#pragma unroll
+            for (int w2 = 0; w2 < RF_THREADS / 32; ++w2) G = fmaxf(G, s_gred[w2]);
+            float acc[4][8], tot[4][8];
 #pragma unroll
             for (int c = 0; c < 4; ++c)
 #pragma unroll
-                for (int jj = 0; jj < 8; ++jj) acc[c][jj] = 0.f;
+                for (int jj = 0; jj < 8; ++jj) acc[c][jj] = tot[c][jj] = 0.f;
             float ring[8];
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) ring[jj] = S.xs[xpad(8 * lane + jj)];
@@ -153,6 +182,15 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
                     }
                     ring[u] = S.xs[xpad(8 * lane + k0 + u + 8)];
                 }
+                if (((k0 + 8) & (RF_SUMBLK - 1)) == 0 || k0 + 8 >= mpad) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+#pragma unroll
+                        for (int jj = 0; jj < 8; ++jj) {
+                            tot[c][jj] += acc[c][jj];
+                            acc[c][jj] = 0.f;
+                        }
+                }
             }
             // ---- epilogue
             bool hit[4] = {false, false, false, false};
@@ -161,19 +199,22 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
                 const int ci = 4 * warp + c;
                 const int w = cw[ci];
                 const float zs = zsum[ci], fc = cf[ci];
+                float cmax = -INFINITY;
 #pragma unroll
                 for (int jj = 0; jj < 8; ++jj) {
                     const int q = 8 * lane + jj;
                     const int j = j0 + q;
                     const int dd = w > j ? w - j : j - w;
                     const bool ok = (j < j_hi) && (dd >= m - 1);
-                    const float rho =
-                        fmaf(fmaf(-zs, S.cmu[q] - sh, acc[c][jj]), S.cinv[q], fc * S.cflt[q]);
+                    // lower bound of the correlation (NaN for a fragile window)
+                    const float rho = fmaf(fmaf(-zs, S.cmu[q] - sh, tot[c][jj]), S.cinv[q],
+                                           fmaf(fc, S.cflt[q], -G));
                     if (ok) {
-                        rmax[c] = fmaxf(rmax[c], rho);
+                        cmax = fmaxf(cmax, rho);
                         hit[c] |= rho > thr;
                     }
                 }
+                rmax[c] = fmaxf(rmax[c], cmax + G); // the interval's middle
             }
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
@@ -215,10 +256,11 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
                                      const int32_t *cand, const int32_t *list,
                                      const int32_t *list_count, PaddiAttemptDev *att,
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
-                                     cudaStream_t st)
+                                     int32_t jb, int32_t je, float thr, float gcap,
+                                     int32_t num_sms, cudaStream_t st)
 {
     if (m > RF_MAXM) return cudaErrorInvalidValue;
+    if ((jb % RF_TW) != 0) return cudaErrorInvalidValue; // chunks on the 256-window grid
     const int mpad = (m + 7) & ~7;
     const size_t smem = sizeof(float) * ((size_t)mpad * RF_TC + (RF_TW + mpad + 8) +
                                          ((RF_TW + mpad + 8) >> 5) + 4 + 3 * RF_TW) + 16;
@@ -230,6 +272,54 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int grid = num_sms * per_sm;
     k_refine_fp32<<<grid, RF_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, att, rho_max,
-                                                  pruned, N, m, jb, je, thr_prune, grid);
+                                                  pruned, N, m, jb, je, thr, grid,
+                                                  paddi_bound_fp32(m).E, gcap);
+    return cudaGetLastError();
+}
+
+PaddiBound paddi_bound_fp32(int m)
+{
+    const double u = std::ldexp(1.0, -24);
+    const int mpad = (m + 7) & ~7;
+    // the dot product in two levels (64 terms, then mpad/64 partials), the z
+    // sum likewise, z's own rounding (x - mu, times inv: 3u), the shifted slice
+    // (u), the epilogue (4u), the FP32 rounding of thr (2u)
+    const double dot = (double)RF_SUMBLK + std::ceil(mpad / (double)RF_SUMBLK) + 1.0;
+    PaddiBound B;
+    B.E = (float)((2.0 * dot + 10.0) * u * 1.01);
+    B.F = 0.f;
+    return B;
+}
+
+// Fragile windows of length m for the FP32 refine's geometry (chunks of 256
+// windows shifted by their first value): the same test as the refine applies.
+__global__ void k_fragile_scan_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
+                                    const float *__restrict__ mu, int32_t N, int32_t m, float E,
+                                    float gcap, int32_t *frag_list, int32_t *frag_count)
+{
+    const int lane = threadIdx.x & 31;
+    for (int j0 = blockIdx.x * blockDim.x; j0 < N; j0 += gridDim.x * blockDim.x) {
+        const int j = j0 + threadIdx.x;
+        bool frag = false;
+        if (j < N) {
+            const float sh = x[j & ~(RF_TW - 1)];
+            frag = paddi::window_bound(wst[j].z, mu[j], sh, (float)m, E, 0.f) > gcap;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, frag);
+        if (bal) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(frag_count, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (frag) frag_list[base + __popc(bal & ((1u << lane) - 1u))] = j;
+        }
+    }
+}
+
+cudaError_t paddi_launch_fragile_scan_fp32(const float *x, const float4 *wst, const float *mu,
+                                           int32_t N, int32_t m, float gcap, int32_t *frag_list,
+                                           int32_t *frag_count, int32_t num_sms, cudaStream_t st)
+{
+    k_fragile_scan_fp32<<<num_sms * 4, 256, 0, st>>>(x, wst, mu, N, m, paddi_bound_fp32(m).E, gcap,
+                                                    frag_list, frag_count);
     return cudaGetLastError();
 }

@@ -50,6 +50,8 @@
 #include <cuda_fp16.h>
 #include <float.h>
 
+#include <cmath>
+
 #include "paddi_internal.cuh"
 
 using paddi::f2ord;
@@ -234,37 +236,63 @@ template <> struct E16<true> {
 
 // ------------------------------------------------------------------ tile prep
 // Block b (windows [2048 b, 2048 b + 2048)): slice x[j0 .. j0 + cnt) minus
-// x[j0], scaled by 2^e (largest magnitude just below 2^14), split into hi
-// and lo halves: bq[b * 2cnt ...] = hi, then lo.  Window data for the
+// its midrange s, scaled by 2^e (largest magnitude just below 2^14), split
+// into hi and lo halves: bq[b * 2cnt ...] = hi, then lo.  Window data for the
 // epilogue in its read layout: shift row s = q % 8, column pair k = q / 16,
 // slot = (q / 8) % 2: wd[s * 129 + k] = {a(slot 0), a(slot 1), b(slot 0), b(slot 1)}
-// with a = inv_j 2^-(8+e) and b = (mu_j - x[j0]) inv_j (zero past N).
+// with a = inv_j 2^-(8+e) and b = (mu_j - s) inv_j (zero past N).
+// Rounding bound: window j's correlations carry at most g_j = window_bound()
+// (E A_j + F inv_j); g_j grows with |mu_j - s| / |x_j - mu_j|, which the
+// midrange keeps small.  A window with g_j > gcap is "fragile": its a is NaN
+// (the epilogue's maxima skip it) and it is appended to frag_list, whose
+// pairs are evaluated in FP64 later.  The largest g_j of the block's other
+// windows, G, is stored in the padding entry wd[128].x: the epilogue
+// subtracts it from every correlation of the tile (a lower bound that is safe
+// to prune on) and adds it back to the maxima it keeps (the middle of the
+// interval, within gcap of every true value).
 constexpr int TP_THREADS = 256;
 
 template <bool BF>
 __global__ void __launch_bounds__(TP_THREADS)
-k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt,
+k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt, int32_t m,
             const float4 *__restrict__ wst, const float *__restrict__ mu, uint16_t *__restrict__ bq,
-            float4 *__restrict__ wdq)
+            float4 *__restrict__ wdq, float E, float Fu, float gcap, int32_t *frag_list,
+            int32_t *frag_count)
 {
     using X = E16<BF>;
-    __shared__ float red[TP_THREADS / 32];
+    __shared__ float red[2][TP_THREADS / 32];
     const int b = blockIdx.x;
     const int64_t j0 = (int64_t)b * UM_TW;
-    const float sh = x[j0];
-    float mx = 0.f;
+    const int64_t N = nser - m + 1;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float lo_v = INFINITY, hi_v = -INFINITY;
     for (int p = threadIdx.x; p < cnt; p += TP_THREADS) {
         const int64_t g = j0 + p;
-        const float v = g < nser ? x[g] - sh : 0.f;
-        mx = fmaxf(mx, fabsf(v));
+        if (g < nser) {
+            lo_v = fminf(lo_v, x[g]);
+            hi_v = fmaxf(hi_v, x[g]);
+        }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    for (int o = 16; o > 0; o >>= 1) {
+        lo_v = fminf(lo_v, __shfl_xor_sync(0xffffffffu, lo_v, o));
+        hi_v = fmaxf(hi_v, __shfl_xor_sync(0xffffffffu, hi_v, o));
+    }
+    if (lane == 0) {
+        red[0][w] = lo_v;
+        red[1][w] = hi_v;
+    }
     __syncthreads();
-    mx = 0.f;
+    lo_v = INFINITY;
+    hi_v = -INFINITY;
 #pragma unroll
-    for (int w = 0; w < TP_THREADS / 32; ++w) mx = fmaxf(mx, red[w]);
+    for (int k = 0; k < TP_THREADS / 32; ++k) {
+        lo_v = fminf(lo_v, red[0][k]);
+        hi_v = fmaxf(hi_v, red[1][k]);
+    }
+    __syncthreads();
+    const float sh = 0.5f * lo_v + 0.5f * hi_v; // midrange (j0 < nser always)
+    const float mx = fmaxf(fabsf(hi_v - sh), fabsf(lo_v - sh));
     int e = 0;
     if (mx > 0.f) {
         int ex;
@@ -288,12 +316,34 @@ k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt,
                  ((uint32_t)reinterpret_cast<const uint16_t &>(l1) << 16);
     }
     float *wf = reinterpret_cast<float *>(wdq + (size_t)b * 8 * WD_ROW);
+    const float F = Fu * mx, fm = (float)m;
+    float gmax = 0.f;
     for (int q = threadIdx.x; q < UM_TW; q += TP_THREADS) {
         const int64_t j = j0 + q; // the padded tail beyond N is zero
         const float iv = wst[j].z, mv = mu[j];
+        const float g = paddi::window_bound(iv, mv, sh, fm, E, F);
+        const bool frag = j < N && g > gcap;
+        if (!frag) gmax = fmaxf(gmax, g);
         const int s = q & 7, i = q >> 3, k = i >> 1, slot = i & 1;
-        wf[(s * WD_ROW + k) * 4 + slot] = iv * dsc;
+        wf[(s * WD_ROW + k) * 4 + slot] = frag ? __int_as_float(0x7fffffff) : iv * dsc;
         wf[(s * WD_ROW + k) * 4 + 2 + slot] = (mv - sh) * iv;
+        // fragile windows in index order within each warp (runs stay contiguous)
+        const unsigned bal = __ballot_sync(0xffffffffu, frag);
+        if (bal) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(frag_count, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (frag) frag_list[base + __popc(bal & ((1u << lane) - 1u))] = (int32_t)j;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) gmax = fmaxf(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
+    if (lane == 0) red[0][w] = gmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float G = 0.f;
+        for (int k = 0; k < TP_THREADS / 32; ++k) G = fmaxf(G, red[0][k]);
+        wf[(0 * WD_ROW + 128) * 4] = G; // padding entry of shift row 0
     }
 }
 
@@ -651,6 +701,10 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                     const bool masked = (j0 + UM_TW > j_hi) ||
                                         (wc > j0 - m + 1 && wc < j0 + UM_TW + m - 1) || fc != 0.f;
                     const float4 *wrow = wd4 + bsh * WD_ROW + 64 * hcol;
+                    // the tile's rounding bound (tile prep): correlations are lowered
+                    // by it for the prune test and raised back for the kept maxima
+                    const float Gt = wd4[128].x;
+                    const float2 ng2 = make_float2(-Gt, -Gt);
                     float tm[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
                     // 4 chunks of 32 columns; the load of chunk cb+1 overlaps the math of cb
                     auto chunk = [&](const uint32_t (&r)[32], int cb) {
@@ -662,7 +716,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                                                               __uint_as_float(r[2 * i2 + 1]));
                                 const float2 rho = __ffma2_rn(
                                     dd, make_float2(wv.x, wv.y),
-                                    __fmul2_rn(nz2, make_float2(wv.z, wv.w)));
+                                    __ffma2_rn(nz2, make_float2(wv.z, wv.w), ng2));
                                 tm[i2 & 3] = fmax3(tm[i2 & 3], rho.x, rho.y);
                             }
                         } else {
@@ -673,7 +727,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                                 const float4 wv = wrow[(32 * cb + i) >> 1];
                                 const float wa = (i & 1) ? wv.y : wv.x;
                                 const float wb = (i & 1) ? wv.w : wv.z;
-                                float rho = fmaf(__uint_as_float(r[i]), wa, -zsc * wb);
+                                float rho = fmaf(__uint_as_float(r[i]), wa, fmaf(-zsc, wb, -Gt));
                                 if (fc != 0.f && wa == 0.f) rho += 1.f; // two flat windows
                                 const int dd = wc > j ? wc - j : j - wc;
                                 if (j < j_hi && dd >= m - 1) tm[i & 3] = fmaxf(tm[i & 3], rho);
@@ -695,7 +749,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                     chunk(rb, 3);
                     float tmax = fmaxf(fmaxf(tm[0], tm[1]), fmaxf(tm[2], tm[3]));
                     if (!rowok) tmax = -INFINITY;
-                    rmax = fmaxf(rmax, tmax);
+                    rmax = fmaxf(rmax, tmax + Gt); // the interval's middle (-inf stays)
                     const unsigned bal = __ballot_sync(0xffffffffu, tmax > thr);
                     if (lane < UM_TC / 4) {
                         const int ci = (UM_TC / 4) * g + lane;
@@ -802,18 +856,46 @@ int64_t paddi_tile_block_elems_max() { return 2 * (int64_t)slice_cnt(UM_KMAX64);
 
 int64_t paddi_tile_wd_entries() { return (int64_t)8 * WD_ROW; }
 
+PaddiBound paddi_bound_tc(int m, bool bf16)
+{
+    const double u = std::ldexp(1.0, -24);
+    const int kp = kpad_of(m);
+    // split representation: z and y each within 2^-22 (FP16) / 2^-16 (BF16) of
+    // their value, the dropped lo*lo term as much again; FP16 z halves below the
+    // normal range: 2^-25 absolute against |z| = 2^8, i.e. 2^-33 sqrt(m) relative
+    const double rep = bf16 ? 3.0 * std::ldexp(1.0, -16)
+                            : 3.0 * std::ldexp(1.0, -22) + std::ldexp(1.0, -33) * std::sqrt((double)m);
+    // the accumulator: one FP32 rounding (taken as 2^-23, truncation) of at most
+    // the sum of |products| per MMA, 3 kp/16 MMAs plus the block sums
+    const double acc = std::ldexp(1.0, -23) * (3.0 * kp / 16.0 + 1.0);
+    // the candidate's split-value sum (2 kp/16 terms per thread + 4 shuffle
+    // levels), its z (two-float centring, scale: 4u), the slice's x - s (u), the
+    // epilogue's a, b and FMA (4u), the FP32 rounding of thr (2u)
+    const double rest = (2.0 * kp / 16.0 + 4.0 + 4.0 + 1.0 + 4.0 + 2.0) * u; // + thr's rounding
+    PaddiBound B;
+    B.E = (float)((rep + acc + rest) * 1.01);
+    // FP16 y halves below the normal range: 2^-25 per scaled value, 2^-(8+e) <=
+    // 2 |x - s|_max 2^-22 of scale, against |z| sqrt(m) 2^8: 2^-38 sqrt(m) |x - s|_max
+    B.F = bf16 ? 0.f : (float)(std::ldexp(1.0, -38) * std::sqrt((double)m) * 1.01);
+    return B;
+}
+
 cudaError_t paddi_launch_tile_prep(bool bf16, const float *x, int64_t n, int32_t m,
                                    const float4 *wst, const float *mu, uint16_t *bq, float4 *wdq,
+                                   float gcap, int32_t *frag_list, int32_t *frag_count,
                                    cudaStream_t st)
 {
     const int kp = kpad_of(m);
     if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
     const int64_t N = n - m + 1;
     const unsigned grid = (unsigned)paddi_tile_blocks(N);
+    const PaddiBound B = paddi_bound_tc(m, bf16);
     if (bf16)
-        k_tile_prep<true><<<grid, TP_THREADS, 0, st>>>(x, n, slice_cnt(kp), wst, mu, bq, wdq);
+        k_tile_prep<true><<<grid, TP_THREADS, 0, st>>>(x, n, slice_cnt(kp), m, wst, mu, bq, wdq,
+                                                       B.E, B.F, gcap, frag_list, frag_count);
     else
-        k_tile_prep<false><<<grid, TP_THREADS, 0, st>>>(x, n, slice_cnt(kp), wst, mu, bq, wdq);
+        k_tile_prep<false><<<grid, TP_THREADS, 0, st>>>(x, n, slice_cnt(kp), m, wst, mu, bq, wdq,
+                                                        B.E, B.F, gcap, frag_list, frag_count);
     return cudaGetLastError();
 }
 

@@ -517,6 +517,8 @@ k_select(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
         res->n_sel = np;
         res->n_recheck = nr;
         res->n_pairs = att->n_pairs;
+        res->n_live = att->n_live;
+        res->p1_walked = att->p1_walked;
         res->status = att->status ? att->status : (s_need ? 2 : 0);
     }
 }

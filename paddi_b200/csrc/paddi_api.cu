@@ -56,6 +56,7 @@ struct paddi_ctx {
     int num_sms = 0;
     cudaStream_t st = nullptr;
     cudaEvent_t ev[8] = {};
+    cudaEvent_t rev[8] = {}; // around each refine round's launch
     // PADDI_TRACE=1 in the environment: one stderr line per attempt with the
     // live-candidate count and the time of every refine round
     bool trace = false;
@@ -93,7 +94,8 @@ struct paddi_ctx {
     unsigned long long *d_nn64 = nullptr;
     PaddiAttemptDev *d_att = nullptr;
     PaddiAttemptResult *d_res = nullptr;
-    int32_t *d_flatcount = nullptr;
+    int32_t *d_flatcount = nullptr; // {flat windows, flat span (2), fragile windows}
+    int32_t *d_frag = nullptr;      // fragile windows of the current length
     PaddiAttemptResult *h_res = nullptr;
     bool umma_ok = false;
     // test hooks (paddi_debug_set): fail the k-th next device allocation; the
@@ -164,6 +166,7 @@ void free_buffers(paddi_ctx *ctx)
     dfree(ctx->d_nn64);
     dfree(ctx->d_list[0]);
     dfree(ctx->d_list[1]);
+    dfree(ctx->d_frag);
     dfree(ctx->d_bq);
     dfree(ctx->d_wdq);
     dfree(ctx->d_pc);
@@ -194,6 +197,7 @@ paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
     CK(dmalloc(ctx, &ctx->d_rho, sizeof(uint32_t) * W));
     CK(dmalloc(ctx, &ctx->d_list[0], sizeof(int32_t) * W));
     CK(dmalloc(ctx, &ctx->d_list[1], sizeof(int32_t) * W));
+    CK(dmalloc(ctx, &ctx->d_frag, sizeof(int32_t) * W));
     if (ctx->umma_ok) {
         const int64_t blocks = paddi_tile_blocks((int64_t)n);
         CK(dmalloc(ctx, &ctx->d_bq, sizeof(uint16_t) * (size_t)(blocks * paddi_tile_block_elems_max())));
@@ -211,8 +215,11 @@ paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
 struct AttemptOut {
     PaddiAttemptResult res;
     float ms_phase1 = 0, ms_refine = 0, ms_select = 0, ms_total = 0;
+    float ms_refine_kernel = 0; // the refine launches alone
+    int nrounds = 0;
     int launches = 0;
     int kernel = PADDI_DIST_FP32;
+    int p1_rows = 0; // rows per phase-1 task
 };
 
 // Refine kernel for length m: the tensor-core split where the length fits
@@ -236,14 +243,21 @@ float guard_of(const paddi_ctx *ctx, int kernel)
 // the tensor-core refine's tile data when that kernel serves this length.
 paddi_status run_stats(paddi_ctx *ctx, const float *x, size_t n, int m, bool tiles = true)
 {
-    // d_flatcount = {flat windows, span of the flat windows (two ints)}
-    CK(cudaMemsetAsync(ctx->d_flatcount, 0, 3 * sizeof(int32_t), ctx->st));
+    // d_flatcount = {flat windows, span of the flat windows (two ints), fragile windows}
+    CK(cudaMemsetAsync(ctx->d_flatcount, 0, 4 * sizeof(int32_t), ctx->st));
     CK(paddi_launch_stats(x, (int64_t)n, m, ctx->d_wst, ctx->d_mu, ctx->d_mu64, ctx->d_inv64,
                           ctx->d_flat, ctx->d_flatcount, ctx->st, ctx->d_flatcount + 1));
     const int kernel = refine_kernel_for(ctx, m);
+    // the refine's per-length data: its tiles (tensor cores) and the windows
+    // whose rounding bound exceeds the guard band (both refine kernels)
     if (tiles && kernel != PADDI_DIST_FP32)
         CK(paddi_launch_tile_prep(kernel == PADDI_DIST_SPLIT_BF16, x, (int64_t)n, m, ctx->d_wst,
-                                  ctx->d_mu, ctx->d_bq, ctx->d_wdq, ctx->st));
+                                  ctx->d_mu, ctx->d_bq, ctx->d_wdq, guard_of(ctx, kernel),
+                                  ctx->d_frag, ctx->d_flatcount + 3, ctx->st));
+    else if (tiles)
+        CK(paddi_launch_fragile_scan_fp32(x, ctx->d_wst, ctx->d_mu, (int32_t)(n - m + 1), m,
+                                          guard_of(ctx, kernel), ctx->d_frag,
+                                          ctx->d_flatcount + 3, ctx->num_sms, ctx->st));
     return PADDI_OK;
 }
 
@@ -266,7 +280,6 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     const int kernel = refine_kernel_for(ctx, m);
     const float guard = guard_of(ctx, kernel);
     const float thr = (float)(1.0 - (double)r2 / (2.0 * (double)m));
-    const float thr_prune = thr + guard;
     // phase-1 rows per task (the reference's SEGMENT_N); validated at the ABI
     // (segment_len_ok), rounded up to a multiple of 8 rows
     int R = (int)ctx->opts.segment_len;
@@ -293,13 +306,16 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     ++launches;
     const bool umma = kernel != PADDI_DIST_FP32;
     out->kernel = kernel;
+    out->p1_rows = R;
     // range edges N/16, N/4, N/2, N: the first rounds prune only a small share
     // each, so they are merged (fewer launches, longer items; a sweep of 4, 5,
     // 6 and 8 rounds picked 4).  The tensor-core refine's tiles sit on a fixed
     // grid: edges are rounded down to multiples of its tile width.
     constexpr int kShifts[3] = {4, 2, 1};
     const int nrounds = N >= (1 << 16) ? 4 : 1;
-    const int tw = umma ? paddi_tile_width() : 1;
+    // round edges on the refine's grid: 2048-window tiles (tensor cores),
+    // 256-window chunks (FP32), so the fragile set depends only on the length
+    const int tw = umma ? paddi_tile_width() : 256;
     int jb = 0;
     for (int rd = 0; rd < nrounds; ++rd) {
         int je = rd == nrounds - 1 ? N : (int)((int64_t)N >> kShifts[rd]) / tw * tw;
@@ -312,18 +328,20 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
                                cudaMemcpyDeviceToDevice, st));
         }
         CK(cudaMemsetAsync(&ctx->d_att->work_next, 0, sizeof(int32_t), st));
+        CK(cudaEventRecord(ctx->rev[2 * rd], st));
         if (umma)
             CK(paddi_launch_refine_umma(kernel == PADDI_DIST_SPLIT_BF16, x, ctx->d_wst, ctx->d_mu,
                                         ctx->d_cand, ctx->d_list[a],
                                         &ctx->d_att->list_count[a], ctx->d_bq, ctx->d_wdq,
                                         ctx->d_att, ctx->d_rho, ctx->d_pruned, N, m, jb, je,
-                                        thr_prune, ctx->num_sms, st, ctx->wait_cycles,
+                                        thr, ctx->num_sms, st, ctx->wait_cycles,
                                         ctx->withhold));
         else
             CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
                                         &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,
-                                        ctx->d_pruned, N, m, jb, je, thr_prune, ctx->num_sms,
+                                        ctx->d_pruned, N, m, jb, je, thr, guard, ctx->num_sms,
                                         st));
+        CK(cudaEventRecord(ctx->rev[2 * rd + 1], st));
         ++launches;
         if (rd + 1 < nrounds) {
             CK(paddi_launch_list_compact(ctx->d_list[a], &ctx->d_att->list_count[a],
@@ -332,6 +350,15 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
             ++launches;
         }
         jb = je;
+    }
+    // the fragile windows (skipped by the refine: their rounding bound exceeds
+    // the guard band) against the candidates the rounds left, in FP64
+    {
+        const int a = (nrounds - 1) & 1;
+        CK(paddi_launch_fragile(x, ctx->d_mu64, ctx->d_inv64, ctx->d_cand, ctx->d_list[a],
+                                &ctx->d_att->list_count[a], ctx->d_pruned, ctx->d_rho,
+                                ctx->d_frag, ctx->d_flatcount + 3, m, thr, ctx->num_sms, st));
+        ++launches;
     }
     CK(cudaEventRecord(ctx->ev[2], st));
     if (ctx->trace) {
@@ -356,6 +383,8 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
                                top_k, ctx->d_flat, ctx->d_res, st));
         launches += 3;
         CK(cudaEventRecord(ctx->ev[3], st));
+        CK(cudaMemcpyAsync(&ctx->d_res->n_fragile, ctx->d_flatcount + 3, sizeof(int32_t),
+                           cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(ctx->h_res, ctx->d_res, sizeof(PaddiAttemptResult),
                            cudaMemcpyDeviceToHost, st));
         if (pass == 0 && next_m > 0) {
@@ -419,6 +448,13 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     }
     CK(cudaEventElapsedTime(&out->ms_phase1, ctx->ev[0], ctx->ev[1]));
     CK(cudaEventElapsedTime(&out->ms_refine, ctx->ev[1], ctx->ev[2]));
+    out->ms_refine_kernel = 0.f;
+    for (int rd = 0; rd < nrounds; ++rd) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->rev[2 * rd], ctx->rev[2 * rd + 1]));
+        out->ms_refine_kernel += ms;
+    }
+    out->nrounds = nrounds;
     CK(cudaEventElapsedTime(&out->ms_select, ctx->ev[2], ctx->ev[3]));
     CK(cudaEventElapsedTime(&out->ms_total, ctx->ev[0], ctx->ev[3]));
     return PADDI_OK;
@@ -449,6 +485,10 @@ void fill_log(paddi_attempt_log *L, int m, float r, float r2, int top_k, const A
     L->ms_select = a.ms_select;
     L->ms_total = a.ms_total + ms_stats;
     L->refine_pairs = (int64_t)a.res.n_pairs;
+    L->refine_live_pairs = (int64_t)a.res.n_live;
+    L->p1_pairs = (int64_t)a.res.p1_walked * (int64_t)a.p1_rows * 256;
+    L->ms_refine_kernel = a.ms_refine_kernel;
+    L->n_fragile = a.res.n_fragile;
     L->n_launches = a.launches + (ms_stats > 0.f ? 1 : 0);
     L->refine_kernel = a.kernel;
     L->r_source = 0;
@@ -864,6 +904,7 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
     }
     bool ok = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) == cudaSuccess;
     for (auto &e : ctx->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+    for (auto &e : ctx->rev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
     {
         const char *tr = std::getenv("PADDI_TRACE");
         ctx->trace = tr && tr[0] && tr[0] != '0';
@@ -876,7 +917,7 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
     }
     ok = ok && cudaMalloc(&ctx->d_att, sizeof(PaddiAttemptDev)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
-    ok = ok && cudaMalloc(&ctx->d_flatcount, 3 * sizeof(int32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&ctx->d_flatcount, 4 * sizeof(int32_t)) == cudaSuccess;
     ok = ok && cudaMallocHost(&ctx->h_res, sizeof(PaddiAttemptResult)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_guide, sizeof(PaddiGuide)) == cudaSuccess;
     ok = ok && cudaMemset(ctx->d_guide, 0, sizeof(PaddiGuide)) == cudaSuccess;
@@ -917,6 +958,8 @@ PADDI_API paddi_status paddi_ctx_destroy(paddi_ctx *ctx)
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : ctx->tev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : ctx->rev)
         if (e) cudaEventDestroy(e);
     if (ctx->d_trace) cudaFree(ctx->d_trace);
     if (ctx->h_trace) cudaFreeHost(ctx->h_trace);

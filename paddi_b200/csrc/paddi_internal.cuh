@@ -48,7 +48,36 @@ __device__ __forceinline__ double ord2d(unsigned long long u)
                                                 : ~u));
 }
 
+// Rounding bound, in correlation units, of a refine kernel's correlation of
+// any candidate with window j whose operand is the series shifted by s:
+//     g_j = E * A_j + F * inv_j,   A_j = |x_j - s| / |x_j - mu_j| = sqrt(1 + m b^2),
+// b = (mu_j - s) inv_j.  E (per kernel and length) bounds the relative error of
+// the dot product with respect to |z| |x_j - s| (|z| = 1), F an absolute error
+// term of the operand's representation.  Explicitly rounded operations, so
+// every kernel that evaluates it for the same window gets the same value.
+__device__ __forceinline__ float window_bound(float inv, float mu, float s, float m, float E,
+                                              float F)
+{
+    const float b = __fmul_rn(__fsub_rn(mu, s), inv);
+    const float A = __fsqrt_rn(__fadd_rn(1.f, __fmul_rn(m, __fmul_rn(b, b))));
+    return __fadd_rn(__fmul_rn(__fmul_rn(E, A), 1.0001f), __fmul_rn(F, inv));
+}
+
 } // namespace paddi
+
+// Bound constants of the refine kernels for length m (see window_bound):
+// E covers the 16-bit split operands (FP16: 2^-22 per value and the dropped
+// lo*lo term; BF16: 2^-16), one FP32 rounding per tensor-core MMA of the
+// accumulator (3 kp/16 MMAs, kp = K padded) and the FP32 arithmetic around it
+// (the candidate's z, the sum of its split values, the epilogue); F covers
+// FP16 lo halves that fall below the normal range (2^-25 absolute per scaled
+// value; F is per unit of the tile's largest |x - s|).  The FP32 CUDA-core
+// refine sums in two levels of 32 terms and has F = 0.
+struct PaddiBound {
+    float E, F;
+};
+PaddiBound paddi_bound_tc(int m, bool bf16);
+PaddiBound paddi_bound_fp32(int m);
 
 // Per-attempt device-side state shared by the kernels of one (m, r) attempt.
 struct PaddiAttemptDev {
@@ -75,6 +104,9 @@ struct PaddiAttemptResult {
     int32_t sel_ind[16];
     float sel_dist[16];
     unsigned long long n_pairs; // refine pairs evaluated
+    unsigned long long n_live;  // of those, pairs of candidates live at the tile's start
+    int32_t p1_walked;          // phase-1 tasks that walked their rows
+    int32_t n_fragile;          // windows the refine left to the FP64 fragile pass
 };
 
 // Incremental FP64 nn of the r policy's bound window (k_guide.cu): the state
@@ -120,13 +152,29 @@ cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
                                  cudaStream_t st);
 
 // Dense refine of the candidates in list[0..*list_count) (positions into
-// cand[]) against the windows [jb, je).
+// cand[]) against the windows [jb, je) (jb a multiple of 256).  thr is the
+// exact threshold 1 - r^2 / (2m): the kernel prunes on lower bounds of the
+// correlations; gcap is the guard band (fragile windows are skipped).
 cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const float *mu,
                                      const int32_t *cand, const int32_t *list,
                                      const int32_t *list_count, PaddiAttemptDev *att,
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
-                                     cudaStream_t st);
+                                     int32_t jb, int32_t je, float thr, float gcap,
+                                     int32_t num_sms, cudaStream_t st);
+
+// Fragile windows of length m in the FP32 refine's geometry, appended to
+// frag_list (frag_count zeroed by the caller).
+cudaError_t paddi_launch_fragile_scan_fp32(const float *x, const float4 *wst, const float *mu,
+                                           int32_t N, int32_t m, float gcap, int32_t *frag_list,
+                                           int32_t *frag_count, int32_t num_sms, cudaStream_t st);
+
+// Exact FP64 correlations of the unpruned candidates of list[0..*list_count)
+// with the fragile windows (k_fragile.cu): prunes and raises rho_max.
+cudaError_t paddi_launch_fragile(const float *x, const double *mu64, const double *inv64,
+                                 const int32_t *cand, const int32_t *list,
+                                 const int32_t *list_count, uint8_t *pruned, uint32_t *rho_max,
+                                 const int32_t *frag, const int32_t *frag_count, int32_t m,
+                                 float thr, int32_t num_sms, cudaStream_t st);
 
 // Tensor-core refine over windows [jb, je) (jb a multiple of the tile width,
 // je too or je = N).  bq / wdq: the per-length tile data of
@@ -150,8 +198,11 @@ int32_t paddi_tile_width();
 int64_t paddi_tile_blocks(int64_t N);
 int64_t paddi_tile_block_elems_max();
 int64_t paddi_tile_wd_entries();
+// Fragile windows (bound above gcap) are appended to frag_list (frag_count
+// zeroed by the caller).
 cudaError_t paddi_launch_tile_prep(bool bf16, const float *x, int64_t n, int32_t m,
                                    const float4 *wst, const float *mu, uint16_t *bq, float4 *wdq,
+                                   float gcap, int32_t *frag_list, int32_t *frag_count,
                                    cudaStream_t st);
 
 cudaError_t paddi_launch_list_init(const PaddiAttemptDev *att, int32_t *list, int32_t *count,

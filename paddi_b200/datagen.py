@@ -17,6 +17,9 @@ Workloads
                      walk + sinusoid mix with 1-3 anomalies of length 32-256.
 * ``ecg_series``     ECG-like beats (Gaussian bumps, period 250 +/- 20) with
                      noise, baseline wander and morphologically altered beats.
+* ``hostile_series`` series built to stress FP32 / 16-bit rounding: near-flat
+                     stretches, a large offset with unit local variance,
+                     integer-quantised values with many ties.
 
 Anomaly positions never overlap; every generator returns the planted
 positions so tests can check that discords land on them.
@@ -33,6 +36,7 @@ __all__ = [
     "batch_series",
     "ecg_series",
     "training_series",
+    "hostile_series",
 ]
 
 
@@ -202,3 +206,54 @@ def ecg_series(n: int = 1 << 27, seed: int = 5, n_altered: int = 64,
     t = np.arange(n, dtype=np.float64)
     x += 0.3 * np.sin(2.0 * np.pi * t / 7919.0) + rng.normal(0.0, 0.05, n)
     return x.astype(np.float32), {"altered_onsets": sorted(int(onsets[b]) for b in altered)}
+
+
+def hostile_series(kind: str, n: int = 1 << 14, seed: int = 0):
+    """Series whose windows have a large |mean - tile level| / std ratio,
+    the case where the distance kernels' rounding is amplified.
+
+    kind: 'near_flat' -> random walk + sinusoid with 6 stretches of 300 points
+                         whose values vary by about 1e-5 of the walk's range
+                         around a level (N(0, 1e-5 * range) on the level);
+          'offset'    -> 1e4 + sin(2 pi t/200) + N(0, 0.3): unit local
+                         variance on a large offset, 4 noise anomalies;
+          'quantised' -> round(2 * random walk) / 2 with 4 planted anomalies:
+                         many ties, flat runs and near-flat windows;
+          'ecg_flat'  -> the ECG-like generator with its beats removed from
+                         4 stretches of 1500 points (a flat, slightly noisy
+                         baseline).
+    Returns (float32 series, info)."""
+    rng = np.random.default_rng(seed)
+    if kind == "near_flat":
+        x = random_walk_sine(n, rng)
+        span = float(x.max() - x.min())
+        lengths = [300] * 6
+        starts = _non_overlapping_starts(n, lengths, rng, margin=300)
+        for s0 in starts:
+            x[s0:s0 + 300] = x[s0] + rng.normal(0.0, 1e-5 * span, 300)
+        return x.astype(np.float32), {"starts": starts, "lengths": lengths}
+    if kind == "offset":
+        t = np.arange(n, dtype=np.float64)
+        x = 1e4 + np.sin(2.0 * np.pi * t / 200.0) + rng.normal(0.0, 0.3, n)
+        lengths = [120] * 4
+        starts = _non_overlapping_starts(n, lengths, rng, margin=120)
+        for s0 in starts:
+            x[s0:s0 + 120] = 1e4 + rng.normal(0.0, 1.5, 120)
+        return x.astype(np.float32), {"starts": starts, "lengths": lengths}
+    if kind == "quantised":
+        x = random_walk_sine(n, rng)
+        lengths = [100] * 4
+        starts = _non_overlapping_starts(n, lengths, rng, margin=100)
+        plant_anomalies(x, starts, lengths, ["noise", "flat", "reverse", "noise"], rng)
+        return (np.round(2.0 * x) / 2.0).astype(np.float32), {"starts": starts,
+                                                               "lengths": lengths}
+    if kind == "ecg_flat":
+        x, info = ecg_series(n=n, seed=seed, n_altered=4)
+        x = x.astype(np.float64)
+        base = np.median(x)
+        lengths = [1500] * 4
+        starts = _non_overlapping_starts(n, lengths, rng, margin=500)
+        for s0 in starts:
+            x[s0:s0 + 1500] = base + rng.normal(0.0, 1e-3, 1500)
+        return x.astype(np.float32), {"starts": starts, "lengths": lengths}
+    raise ValueError(kind)

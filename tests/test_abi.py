@@ -34,7 +34,7 @@ def test_bindings_cover_the_header():
 
 def test_abi_version_and_status_strings():
     L = P.lib()
-    assert L.paddi_abi_version() == 1
+    assert L.paddi_abi_version() == 2
     assert P.status_string(P.PADDI_OK) == "ok"
     assert "invalid" in P.status_string(P.PADDI_ERR_INVALID_ARG)
     assert P.status_string(12345) == "unknown status"
