@@ -236,14 +236,18 @@ template <> struct E16<true> {
 
 // ------------------------------------------------------------------ tile prep
 // Block b (windows [2048 b, 2048 b + 2048)): slice x[j0 .. j0 + cnt) minus
-// its midrange s, scaled by 2^e (largest magnitude just below 2^14), split
+// its level s, scaled by 2^e (largest magnitude just below 2^14), split
 // into hi and lo halves: bq[b * 2cnt ...] = hi, then lo.  Window data for the
 // epilogue in its read layout: shift row s = q % 8, column pair k = q / 16,
 // slot = (q / 8) % 2: wd[s * 129 + k] = {a(slot 0), a(slot 1), b(slot 0), b(slot 1)}
 // with a = inv_j 2^-(8+e) and b = (mu_j - s) inv_j (zero past N).
 // Rounding bound: window j's correlations carry at most g_j = window_bound()
-// (E A_j + F inv_j); g_j grows with |mu_j - s| / |x_j - mu_j|, which the
-// midrange keeps small.  A window with g_j > gcap is "fragile": its a is NaN
+// (E A_j + F inv_j); g_j grows with |mu_j - s| / |x_j - mu_j|.  The level s
+// is the mean of the block's window means weighted by 1 / |x_j - mu_j|^2 (it
+// minimises the sum of (mu_j - s)^2 / |x_j - mu_j|^2, so the low-variance
+// windows, where the amplification is large, pull it towards their level);
+// the slice's midrange if no window has a norm.  A window with g_j > gcap is
+// "fragile": its a is NaN
 // (the epilogue's maxima skip it) and it is appended to frag_list, whose
 // pairs are evaluated in FP64 later.  The largest g_j of the block's other
 // windows, G, is stored in the padding entry wd[128].x: the epilogue
@@ -260,11 +264,21 @@ k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt, int32_t m,
             int32_t *frag_count)
 {
     using X = E16<BF>;
-    __shared__ float red[2][TP_THREADS / 32];
+    __shared__ float red[4][TP_THREADS / 32];
     const int b = blockIdx.x;
     const int64_t j0 = (int64_t)b * UM_TW;
     const int64_t N = nser - m + 1;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float sw = 0.f, swm = 0.f; // sums of 1/|x_j - mu_j|^2 and mu_j/|x_j - mu_j|^2
+    for (int q = threadIdx.x; q < UM_TW; q += TP_THREADS) {
+        const int64_t j = j0 + q;
+        if (j < N) {
+            const float iv = wst[j].z;
+            const float wgt = fminf(iv * iv, 1e30f);
+            sw += wgt;
+            swm = fmaf(wgt, mu[j], swm);
+        }
+    }
     float lo_v = INFINITY, hi_v = -INFINITY;
     for (int p = threadIdx.x; p < cnt; p += TP_THREADS) {
         const int64_t g = j0 + p;
@@ -277,21 +291,33 @@ k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt, int32_t m,
     for (int o = 16; o > 0; o >>= 1) {
         lo_v = fminf(lo_v, __shfl_xor_sync(0xffffffffu, lo_v, o));
         hi_v = fmaxf(hi_v, __shfl_xor_sync(0xffffffffu, hi_v, o));
+        sw += __shfl_xor_sync(0xffffffffu, sw, o);
+        swm += __shfl_xor_sync(0xffffffffu, swm, o);
     }
     if (lane == 0) {
         red[0][w] = lo_v;
         red[1][w] = hi_v;
+        red[2][w] = sw;
+        red[3][w] = swm;
     }
     __syncthreads();
     lo_v = INFINITY;
     hi_v = -INFINITY;
+    sw = 0.f;
+    swm = 0.f;
 #pragma unroll
     for (int k = 0; k < TP_THREADS / 32; ++k) {
         lo_v = fminf(lo_v, red[0][k]);
         hi_v = fmaxf(hi_v, red[1][k]);
+        sw += red[2][k];
+        swm += red[3][k];
     }
     __syncthreads();
-    const float sh = 0.5f * lo_v + 0.5f * hi_v; // midrange (j0 < nser always)
+    float sh = 0.5f * lo_v + 0.5f * hi_v; // midrange (j0 < nser always)
+    if (sw > 0.f) {
+        const float lv = swm / sw; // the weighted level, kept inside the slice's range
+        if (isfinite(lv)) sh = fminf(fmaxf(lv, lo_v), hi_v);
+    }
     const float mx = fmaxf(fabsf(hi_v - sh), fabsf(lo_v - sh));
     int e = 0;
     if (mx > 0.f) {

@@ -354,11 +354,13 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     // the fragile windows (skipped by the refine: their rounding bound exceeds
     // the guard band) against the candidates the rounds left, in FP64
     {
-        const int a = (nrounds - 1) & 1;
-        CK(paddi_launch_fragile(x, ctx->d_mu64, ctx->d_inv64, ctx->d_cand, ctx->d_list[a],
-                                &ctx->d_att->list_count[a], ctx->d_pruned, ctx->d_rho,
+        const int a = (nrounds - 1) & 1, b = a ^ 1;
+        CK(paddi_launch_list_compact(ctx->d_list[a], &ctx->d_att->list_count[a], ctx->d_pruned,
+                                     ctx->d_list[b], &ctx->d_att->list_count[b], st));
+        CK(paddi_launch_fragile(x, ctx->d_mu64, ctx->d_inv64, ctx->d_cand, ctx->d_list[b],
+                                &ctx->d_att->list_count[b], ctx->d_pruned, ctx->d_rho,
                                 ctx->d_frag, ctx->d_flatcount + 3, m, thr, ctx->num_sms, st));
-        ++launches;
+        launches += 2;
     }
     CK(cudaEventRecord(ctx->ev[2], st));
     if (ctx->trace) {
