@@ -272,6 +272,47 @@ paddi_status paddi_model_grad(paddi_ctx *ctx, const float *X, const float *Y, ui
 paddi_status paddi_model_predict(paddi_ctx *ctx, const float *X, uint32_t n,
                                  const float *params, int32_t bf16, float *Y);
 
+/* ---------------------------------------------------------------- shards
+ * One attempt (length m, threshold r2 = r*r) split over the GPUs of a job,
+ * one process per GPU, every process holding the whole series.  Replaces the
+ * reference's fragment split with halos (src/data_preparation.cuh:30-75), its
+ * candidate exchange (src/MPI_transfers.hpp:29-84) and the minimum over GPUs
+ * of the candidates' distances (src/sets_processing.hpp:152-164); the two
+ * exchanges are the caller's (NCCL through torch.distributed, MPI, ...):
+ *   1. paddi_shard_phase1: statistics of length m, then phase 1 on the rows
+ *      [row_lo, row_hi) (their neighbours anywhere); writes the alive flags
+ *      (uint8, 1 = not pruned) of all N = n - m + 1 windows to d_alive.
+ *      Exchange: element-wise minimum of d_alive over the GPUs.
+ *   2. paddi_shard_refine: the candidates of the combined flags against the
+ *      windows [col_lo, col_hi) (col_lo a multiple of 2048; col_hi too, or N);
+ *      writes per candidate its window (d_ind), its correlation maximum as an
+ *      order-preserving uint32 image (d_rho: unsigned max = float max) and its
+ *      pruned flag (d_pruned), *n_cand of them (at most cap).  Every GPU has the
+ *      same candidate set, in an order of its own.
+ *      Exchange: per window, the maximum of d_rho and of d_pruned over the GPUs.
+ *   3. paddi_shard_select: classification, FP64 recheck and top-k of the
+ *      merged candidates (count of them); the same result on every GPU.
+ * The three steps run in this order on one context for one (m, r2); d_series
+ * is a device pointer to n values.  log (optional) receives the attempt's row.
+ */
+paddi_status paddi_shard_phase1(paddi_ctx *ctx, const float *d_series, size_t n, uint32_t m,
+                                float r2, size_t row_lo, size_t row_hi, uint8_t *d_alive);
+paddi_status paddi_shard_refine(paddi_ctx *ctx, const float *d_series, size_t n, uint32_t m,
+                                float r2, const uint8_t *d_alive, size_t col_lo, size_t col_hi,
+                                int32_t *d_ind, uint32_t *d_rho, uint8_t *d_pruned, uint32_t cap,
+                                uint32_t *n_cand);
+paddi_status paddi_shard_select(paddi_ctx *ctx, const float *d_series, size_t n, uint32_t m,
+                                float r2, const int32_t *d_ind, const uint32_t *d_rho,
+                                const uint8_t *d_pruned, uint32_t count, uint32_t top_k,
+                                paddi_discord *out, uint32_t *n_out, paddi_attempt_log *log);
+
+/* The reference's MERLIN r-schedule (src/main.cu:136-233) as pure host
+ * functions, for drivers outside the library: the first r of length minL + j
+ * from the top-1 distances of the previous lengths (out[0..j-1]) with its
+ * decrement *S, and the r after an attempt without a discord. */
+float paddi_merlin_first_r(const paddi_discord *out, uint32_t j, uint32_t minL, float *S);
+float paddi_merlin_lower(float r, uint32_t j, float S);
+
 /* ------------------------------------------------------------------ test hooks
  * No counterpart in the reference, which exits the process on any CUDA error
  * (src/common.h:6-16).  These make a failure happen on the host, or make a

@@ -143,6 +143,17 @@ _SIGS = {
                           C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "paddi_model_predict": ([C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int32,
                              C.c_void_p], C.c_int),
+    "paddi_shard_phase1": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_float,
+                            C.c_size_t, C.c_size_t, C.c_void_p], C.c_int),
+    "paddi_shard_refine": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_float,
+                            C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p,
+                            C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
+    "paddi_shard_select": ([C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_float,
+                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                            C.POINTER(_Discord), C.POINTER(C.c_uint32), C.POINTER(_Log)], C.c_int),
+    "paddi_merlin_first_r": ([C.POINTER(_Discord), C.c_uint32, C.c_uint32,
+                              C.POINTER(C.c_float)], C.c_float),
+    "paddi_merlin_lower": ([C.c_float, C.c_uint32, C.c_float], C.c_float),
     "paddi_debug_set": ([C.c_void_p, C.c_int32, C.c_int64], C.c_int),
     "paddi_debug_get": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int64)], C.c_int),
 }

@@ -39,7 +39,8 @@ k_fragile(const float *__restrict__ x, const double *__restrict__ mu64,
           const double *__restrict__ inv64, const int32_t *__restrict__ cand,
           const int32_t *__restrict__ list, const int32_t *__restrict__ list_count,
           uint8_t *pruned, uint32_t *rho_max, const int32_t *__restrict__ frag,
-          const int32_t *__restrict__ frag_count, int32_t m, float thr)
+          const int32_t *__restrict__ frag_count, int32_t m, float thr, int32_t col_lo,
+          int32_t col_hi)
 {
     extern __shared__ __align__(16) double fg_a[]; // [FG_CAND][mpad]: centred candidates
     __shared__ int cw[FG_CAND], cp[FG_CAND], live[FG_CAND];
@@ -76,8 +77,8 @@ k_fragile(const float *__restrict__ x, const double *__restrict__ mu64,
 #pragma unroll
         for (int c = 0; c < FG_CAND; ++c) best[c] = -INFINITY;
         const int fi = chunk * FG_THREADS + t;
-        if (fi < F) {
-            const int f = frag[fi];
+        const int f = fi < F ? frag[fi] : -1;
+        if (f >= col_lo && f < col_hi) {
             const double mf = mu64[f], ivf = inv64[f];
             double acc[FG_CAND];
 #pragma unroll
@@ -125,7 +126,8 @@ cudaError_t paddi_launch_fragile(const float *x, const double *mu64, const doubl
                                  const int32_t *cand, const int32_t *list,
                                  const int32_t *list_count, uint8_t *pruned, uint32_t *rho_max,
                                  const int32_t *frag, const int32_t *frag_count, int32_t m,
-                                 float thr, int32_t num_sms, cudaStream_t st)
+                                 float thr, int32_t col_lo, int32_t col_hi, int32_t num_sms,
+                                 cudaStream_t st)
 {
     if (m > FG_MAXM) return cudaErrorInvalidValue;
     const int mpad = (m + FG_UNROLL - 1) / FG_UNROLL * FG_UNROLL;
@@ -133,6 +135,7 @@ cudaError_t paddi_launch_fragile(const float *x, const double *mu64, const doubl
     cudaError_t e = paddi_raise_smem_limit((const void *)k_fragile, smem);
     if (e != cudaSuccess) return e;
     k_fragile<<<num_sms * 2, FG_THREADS, smem, st>>>(x, mu64, inv64, cand, list, list_count,
-                                                    pruned, rho_max, frag, frag_count, m, thr);
+                                                    pruned, rho_max, frag, frag_count, m, thr,
+                                                    col_lo, col_hi);
     return cudaGetLastError();
 }

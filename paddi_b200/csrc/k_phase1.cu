@@ -198,7 +198,8 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
 __global__ void __launch_bounds__(P1_THREADS, 16)
 k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const float *__restrict__ mu,
          const double *__restrict__ mu64, uint8_t *alive, int32_t N, int32_t m, int32_t R,
-         int32_t max_chunks, float thr, int32_t *task_counter, int32_t *walked)
+         int32_t max_chunks, float thr, int32_t row_lo, int32_t row_hi, int32_t *task_counter,
+         int32_t *walked)
 {
     extern __shared__ __align__(16) unsigned char p1_smem[];
     const int mpad = (m + 7) & ~7;
@@ -217,7 +218,7 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
 
     const int t = threadIdx.x;
     const int c0 = P1_GPT * t;
-    const int nseg = (N + R - 1) / R;
+    const int nseg = (row_hi - row_lo + R - 1) / R; // segments of the row range
     const int total = nseg * max_chunks;
     const float sqrtm = sqrtf((float)m) * (1.f + 2.f * kU);
     // rounding-bound constants of the start dot products
@@ -230,8 +231,8 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
         __syncwarp();
         if (task >= total) break;
         const int chunk = task / nseg, seg = task - chunk * nseg;
-        const int i0 = seg * R;
-        const int rows = min(R, N - i0);
+        const int i0 = row_lo + seg * R;
+        const int rows = min(R, row_hi - i0);
         const int d0 = (m - 1) + chunk * P1_D;
         if (i0 + d0 >= N) continue; // no admissible pair in this task
         if (chunk > 0) { // continue only while some row is still a candidate
@@ -378,11 +379,12 @@ size_t paddi_phase1_smem(int R, int m)
 
 cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const float *mu,
                                     const double *mu64, uint8_t *alive, int32_t N, int32_t m,
-                                    int32_t R, int32_t max_chunks, float thr,
-                                    int32_t *task_counter, int32_t *walked, int32_t num_sms,
-                                    cudaStream_t st)
+                                    int32_t R, int32_t max_chunks, float thr, int32_t row_lo,
+                                    int32_t row_hi, int32_t *task_counter, int32_t *walked,
+                                    int32_t num_sms, cudaStream_t st)
 {
-    if (R < 64 || R > 4096 || (R & 7) || m > P1_MAXM || max_chunks < 1)
+    if (R < 64 || R > 4096 || (R & 7) || m > P1_MAXM || max_chunks < 1 || row_lo < 0 ||
+        row_hi > N || row_lo >= row_hi)
         return cudaErrorInvalidValue;
     const size_t smem = paddi_phase1_smem(R, m);
     cudaError_t e = paddi_raise_smem_limit((const void *)k_phase1, smem);
@@ -391,10 +393,10 @@ cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const flo
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase1, P1_THREADS, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    const int nseg = (N + R - 1) / R;
+    const int nseg = (row_hi - row_lo + R - 1) / R;
     int grid = num_sms * per_sm;
     if (grid > nseg * max_chunks) grid = nseg * max_chunks;
     k_phase1<<<grid, P1_THREADS, smem, st>>>(x, wst, mu, mu64, alive, N, m, R, max_chunks, thr,
-                                             task_counter, walked);
+                                             row_lo, row_hi, task_counter, walked);
     return cudaGetLastError();
 }

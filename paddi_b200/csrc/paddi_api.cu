@@ -261,65 +261,49 @@ paddi_status run_stats(paddi_ctx *ctx, const float *x, size_t n, int m, bool til
     return PADDI_OK;
 }
 
-// One (m, r2) attempt on the statistics currently in the context.
-// known_w >= 0: window whose exact FP64 nn at this length is already known
-// (its ordered image known_ord, from the guide kernel); the recheck skips it.
+// Queues the statistics of length m and the bound (see the definition).
+// known_w >= 0 (in the attempt functions): window whose exact FP64 nn at this
+// length is already known (its ordered image known_ord, from the guide
+// kernel); the recheck skips it.
 paddi_status enqueue_prep(paddi_ctx *ctx, const float *x, size_t n, int m, bool guided,
                           int32_t w_host);
 
-// next_m > 0: the statistics (and, with next_guided, the bound) of length
-// next_m are queued behind the attempt, before its result is synced, so the
-// host waits once per length; *spec_out then tells whether the statistics
-// now hold next_m (not when the selection had to be redone).
-paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float r2, int top_k,
-                         AttemptOut *out, int32_t known_w = -1, unsigned long long known_ord = 0,
-                         int next_m = 0, bool next_guided = false, bool *spec_out = nullptr)
+// Phase-1 rows per task (the reference's SEGMENT_N); validated at the ABI
+// (segment_len_ok), rounded up to a multiple of 8 rows.
+int p1_rows_of(const paddi_ctx *ctx)
 {
-    bool spec = false;
-    const int32_t N = (int32_t)(n - m + 1);
-    const int kernel = refine_kernel_for(ctx, m);
-    const float guard = guard_of(ctx, kernel);
-    const float thr = (float)(1.0 - (double)r2 / (2.0 * (double)m));
-    // phase-1 rows per task (the reference's SEGMENT_N); validated at the ABI
-    // (segment_len_ok), rounded up to a multiple of 8 rows
     int R = (int)ctx->opts.segment_len;
     if (R <= 0) R = 256;
-    R = (R + 7) & ~7;
-    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 12;
+    return (R + 7) & ~7;
+}
+
+// The correlation threshold of r^2 at length m: d < r^2 <=> rho > thr.
+float thr_of(float r2, int m) { return (float)(1.0 - (double)r2 / (2.0 * (double)m)); }
+
+// Refine rounds of the compacted candidates against the windows [col_lo,
+// col_hi) (col_lo on the refine's grid), then the FP64 pass over the fragile
+// windows of that range.  Rounds over growing window ranges (1/16, 1/4, 1/2,
+// all of the range; a sweep of 4 to 8 rounds picked 4); survivors are
+// re-compacted between rounds so every tile is dense with live candidates.
+paddi_status refine_rounds(paddi_ctx *ctx, const float *x, int32_t N, int m, int kernel,
+                           float thr, float guard, int32_t col_lo, int32_t col_hi,
+                           int *launches, int *nrounds_out)
+{
     cudaStream_t st = ctx->st;
-    CK(cudaEventRecord(ctx->ev[0], st));
-    CK(cudaMemsetAsync(ctx->d_alive, 1, (size_t)N, st));
-    CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
-    int launches = 0;
-    CK(paddi_launch_phase1_dev(x, ctx->d_wst, ctx->d_mu, ctx->d_mu64, ctx->d_alive, N, m, R,
-                               chunks, thr, &ctx->d_att->task_next, &ctx->d_att->p1_walked,
-                               ctx->num_sms, st));
-    ++launches;
-    CK(cudaEventRecord(ctx->ev[1], st));
-    CK(paddi_launch_compact(ctx->d_alive, N, ctx->d_cand, ctx->d_rho, ctx->d_pruned,
-                            ctx->d_rcslot, ctx->d_att, ctx->d_flat, ctx->d_flatcount + 1, m,
-                            r2 > 0.f, st));
-    ++launches;
-    // refine rounds over growing window ranges; survivors are re-compacted
-    // between rounds so every tile is dense with live candidates
     CK(paddi_launch_list_init(ctx->d_att, ctx->d_list[0], &ctx->d_att->list_count[0], st));
-    ++launches;
+    ++*launches;
     const bool umma = kernel != PADDI_DIST_FP32;
-    out->kernel = kernel;
-    out->p1_rows = R;
-    // range edges N/16, N/4, N/2, N: the first rounds prune only a small share
-    // each, so they are merged (fewer launches, longer items; a sweep of 4, 5,
-    // 6 and 8 rounds picked 4).  The tensor-core refine's tiles sit on a fixed
-    // grid: edges are rounded down to multiples of its tile width.
     constexpr int kShifts[3] = {4, 2, 1};
-    const int nrounds = N >= (1 << 16) ? 4 : 1;
+    const int32_t range = col_hi - col_lo;
+    const int nrounds = range >= (1 << 16) ? 4 : 1;
     // round edges on the refine's grid: 2048-window tiles (tensor cores),
     // 256-window chunks (FP32), so the fragile set depends only on the length
     const int tw = umma ? paddi_tile_width() : 256;
-    int jb = 0;
+    int jb = col_lo;
     for (int rd = 0; rd < nrounds; ++rd) {
-        int je = rd == nrounds - 1 ? N : (int)((int64_t)N >> kShifts[rd]) / tw * tw;
-        if (je > N) je = N;
+        int je = rd == nrounds - 1 ? col_hi
+                                   : col_lo + (int)((int64_t)range >> kShifts[rd]) / tw * tw;
+        if (je > col_hi) je = col_hi;
         if (je < jb) je = jb;
         const int a = rd & 1, b = a ^ 1;
         if (ctx->trace) {
@@ -342,36 +326,41 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
                                         ctx->d_pruned, N, m, jb, je, thr, guard, ctx->num_sms,
                                         st));
         CK(cudaEventRecord(ctx->rev[2 * rd + 1], st));
-        ++launches;
+        ++*launches;
         if (rd + 1 < nrounds) {
             CK(paddi_launch_list_compact(ctx->d_list[a], &ctx->d_att->list_count[a],
                                          ctx->d_pruned, ctx->d_list[b],
                                          &ctx->d_att->list_count[b], st));
-            ++launches;
+            ++*launches;
         }
         jb = je;
     }
     // the fragile windows (skipped by the refine: their rounding bound exceeds
     // the guard band) against the candidates the rounds left, in FP64
-    {
-        const int a = (nrounds - 1) & 1, b = a ^ 1;
-        CK(paddi_launch_list_compact(ctx->d_list[a], &ctx->d_att->list_count[a], ctx->d_pruned,
-                                     ctx->d_list[b], &ctx->d_att->list_count[b], st));
-        CK(paddi_launch_fragile(x, ctx->d_mu64, ctx->d_inv64, ctx->d_cand, ctx->d_list[b],
-                                &ctx->d_att->list_count[b], ctx->d_pruned, ctx->d_rho,
-                                ctx->d_frag, ctx->d_flatcount + 3, m, thr, ctx->num_sms, st));
-        launches += 2;
-    }
-    CK(cudaEventRecord(ctx->ev[2], st));
-    if (ctx->trace) {
-        CK(cudaEventRecord(ctx->tev[nrounds], st));
-        CK(cudaMemcpyAsync(ctx->d_trace + 7, &ctx->d_att->p1_walked, sizeof(int32_t),
-                           cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(ctx->h_trace64, &ctx->d_att->n_pairs, 2 * sizeof(unsigned long long),
-                           cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(ctx->h_trace, ctx->d_trace, sizeof(int32_t) * 8,
-                           cudaMemcpyDeviceToHost, st));
-    }
+    const int a = (nrounds - 1) & 1, b = a ^ 1;
+    CK(paddi_launch_list_compact(ctx->d_list[a], &ctx->d_att->list_count[a], ctx->d_pruned,
+                                 ctx->d_list[b], &ctx->d_att->list_count[b], st));
+    CK(paddi_launch_fragile(x, ctx->d_mu64, ctx->d_inv64, ctx->d_cand, ctx->d_list[b],
+                            &ctx->d_att->list_count[b], ctx->d_pruned, ctx->d_rho, ctx->d_frag,
+                            ctx->d_flatcount + 3, m, thr, col_lo, col_hi, ctx->num_sms, st));
+    *launches += 2;
+    *nrounds_out = nrounds;
+    return PADDI_OK;
+}
+
+// Classification, FP64 recheck and top-k selection of the refined
+// candidates, redone (at most 6 passes) when the recheck queue overflows or a
+// pick lacks an exact value.  next_m > 0: the statistics (and, with
+// next_guided, the bound) of length next_m are queued behind the first pass,
+// before its result is synced; *spec tells whether they were.
+paddi_status select_passes(paddi_ctx *ctx, const float *x, size_t n, int m, float r2,
+                           float guard, int top_k, int32_t known_w, unsigned long long known_ord,
+                           int next_m, bool next_guided, bool *spec, int *launches)
+{
+    const int32_t N = (int32_t)(n - m + 1);
+    const float thr = thr_of(r2, m);
+    cudaStream_t st = ctx->st;
+    *spec = false;
     float widen = 2.f;
     for (int pass = 0; pass < 6; ++pass) {
         CK(paddi_launch_finalize(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned, m, r2, thr,
@@ -383,7 +372,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         CK(paddi_launch_select(ctx->d_cand, ctx->d_att, ctx->d_rho, ctx->d_pruned,
                                ctx->d_recheck, ctx->d_rcslot, ctx->d_nn64, m, r2, thr, guard,
                                top_k, ctx->d_flat, ctx->d_res, st));
-        launches += 3;
+        *launches += 3;
         CK(cudaEventRecord(ctx->ev[3], st));
         CK(cudaMemcpyAsync(&ctx->d_res->n_fragile, ctx->d_flatcount + 3, sizeof(int32_t),
                            cudaMemcpyDeviceToDevice, st));
@@ -392,7 +381,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         if (pass == 0 && next_m > 0) {
             paddi_status s = enqueue_prep(ctx, x, n, next_m, next_guided, -1);
             if (s != PADDI_OK) return s;
-            spec = true;
+            *spec = true;
         }
         CK(cudaStreamSynchronize(st));
         ctx->last_passes = pass + 1;
@@ -414,10 +403,10 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
         } else {
             break;
         }
-        if (spec) { // the redo needs this length's statistics back
+        if (*spec) { // the redo needs this length's statistics back
             paddi_status s = run_stats(ctx, x, n, m);
             if (s != PADDI_OK) return s;
-            spec = false;
+            *spec = false;
         }
         CK(cudaMemsetAsync(&ctx->d_att->recheck_next, 0, sizeof(int32_t), st));
         CK(cudaMemsetAsync(&ctx->d_att->status, 0, sizeof(int32_t), st));
@@ -432,6 +421,57 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
                         ", widen=" + std::to_string(widen) + ")");
     if (ctx->h_res->status != 0)
         return fail(ctx, PADDI_ERR_INTERNAL_LIMIT, "top-k selection did not settle");
+    return PADDI_OK;
+}
+
+// One (m, r2) attempt on the statistics currently in the context.
+// next_m > 0: the statistics (and, with next_guided, the bound) of length
+// next_m are queued behind the attempt, before its result is synced, so the
+// host waits once per length; *spec_out then tells whether the statistics
+// now hold next_m (not when the selection had to be redone).
+paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float r2, int top_k,
+                         AttemptOut *out, int32_t known_w = -1, unsigned long long known_ord = 0,
+                         int next_m = 0, bool next_guided = false, bool *spec_out = nullptr)
+{
+    const int32_t N = (int32_t)(n - m + 1);
+    const int kernel = refine_kernel_for(ctx, m);
+    const float guard = guard_of(ctx, kernel);
+    const float thr = thr_of(r2, m);
+    const int R = p1_rows_of(ctx);
+    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 12;
+    cudaStream_t st = ctx->st;
+    CK(cudaEventRecord(ctx->ev[0], st));
+    CK(cudaMemsetAsync(ctx->d_alive, 1, (size_t)N, st));
+    CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
+    int launches = 0;
+    CK(paddi_launch_phase1_dev(x, ctx->d_wst, ctx->d_mu, ctx->d_mu64, ctx->d_alive, N, m, R,
+                               chunks, thr, 0, N, &ctx->d_att->task_next,
+                               &ctx->d_att->p1_walked, ctx->num_sms, st));
+    ++launches;
+    CK(cudaEventRecord(ctx->ev[1], st));
+    CK(paddi_launch_compact(ctx->d_alive, N, ctx->d_cand, ctx->d_rho, ctx->d_pruned,
+                            ctx->d_rcslot, ctx->d_att, ctx->d_flat, ctx->d_flatcount + 1, m,
+                            r2 > 0.f, st));
+    ++launches;
+    out->kernel = kernel;
+    out->p1_rows = R;
+    int nrounds = 0;
+    paddi_status s = refine_rounds(ctx, x, N, m, kernel, thr, guard, 0, N, &launches, &nrounds);
+    if (s != PADDI_OK) return s;
+    CK(cudaEventRecord(ctx->ev[2], st));
+    if (ctx->trace) {
+        CK(cudaEventRecord(ctx->tev[nrounds], st));
+        CK(cudaMemcpyAsync(ctx->d_trace + 7, &ctx->d_att->p1_walked, sizeof(int32_t),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ctx->h_trace64, &ctx->d_att->n_pairs, 2 * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ctx->h_trace, ctx->d_trace, sizeof(int32_t) * 8,
+                           cudaMemcpyDeviceToHost, st));
+    }
+    bool spec = false;
+    s = select_passes(ctx, x, n, m, r2, guard, top_k, known_w, known_ord, next_m, next_guided,
+                      &spec, &launches);
+    if (s != PADDI_OK) return s;
     out->res = *ctx->h_res;
     out->launches = launches;
     if (spec_out) *spec_out = spec;
@@ -445,8 +485,9 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
             CK(cudaEventElapsedTime(&ms, ctx->tev[rd], ctx->tev[rd + 1]));
             line += " " + std::to_string(ctx->h_trace[rd]) + "/" + std::to_string(ms);
         }
-        std::fprintf(stderr, "%s disc=%lld pairs=%llu live=%llu\n", line.c_str(),
-                     (long long)ctx->h_res->n_disc, ctx->h_trace64[0], ctx->h_trace64[1]);
+        std::fprintf(stderr, "%s disc=%lld pairs=%llu live=%llu fragile=%d\n", line.c_str(),
+                     (long long)ctx->h_res->n_disc, ctx->h_trace64[0], ctx->h_trace64[1],
+                     ctx->h_res->n_fragile);
     }
     CK(cudaEventElapsedTime(&out->ms_phase1, ctx->ev[0], ctx->ev[1]));
     CK(cudaEventElapsedTime(&out->ms_refine, ctx->ev[1], ctx->ev[2]));
@@ -1148,6 +1189,144 @@ PADDI_API paddi_status paddi_do_pd3(paddi_ctx *ctx, const float *d_T, size_t n, 
     }
     if (n_cand) *n_cand = a.res.n_cand;
     return PADDI_OK;
+}
+
+// ==================================================================== shards
+PADDI_API paddi_status paddi_shard_phase1(paddi_ctx *ctx, const float *d_series, size_t n,
+                                          uint32_t m, float r2, size_t row_lo, size_t row_hi,
+                                          uint8_t *d_alive)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!d_series || !d_alive || !valid_lengths(n, m, m) || !(r2 >= 0.f))
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "shard_phase1: invalid series, length or r2");
+    const size_t N = n - m + 1;
+    if (row_lo >= row_hi || row_hi > N)
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "shard_phase1: empty or out-of-range rows");
+    CK(cudaSetDevice(ctx->device));
+    paddi_status s = ensure_capacity(ctx, n);
+    if (s != PADDI_OK) return s;
+    s = run_stats(ctx, d_series, n, (int)m);
+    if (s != PADDI_OK) return s;
+    cudaStream_t st = ctx->st;
+    CK(cudaMemsetAsync(d_alive, 1, N, st));
+    CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
+    const int chunks = ctx->opts.phase1_chunks ? (int)ctx->opts.phase1_chunks : 12;
+    CK(paddi_launch_phase1_dev(d_series, ctx->d_wst, ctx->d_mu, ctx->d_mu64, d_alive, (int32_t)N,
+                               (int)m, p1_rows_of(ctx), chunks, thr_of(r2, (int)m),
+                               (int32_t)row_lo, (int32_t)row_hi, &ctx->d_att->task_next,
+                               &ctx->d_att->p1_walked, ctx->num_sms, st));
+    CK(cudaStreamSynchronize(st));
+    return PADDI_OK;
+}
+
+PADDI_API paddi_status paddi_shard_refine(paddi_ctx *ctx, const float *d_series, size_t n,
+                                          uint32_t m, float r2, const uint8_t *d_alive,
+                                          size_t col_lo, size_t col_hi, int32_t *d_ind,
+                                          uint32_t *d_rho, uint8_t *d_pruned, uint32_t cap,
+                                          uint32_t *n_cand)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!d_series || !d_alive || !d_ind || !d_rho || !d_pruned || !n_cand ||
+        !valid_lengths(n, m, m) || !(r2 >= 0.f))
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "shard_refine: invalid argument");
+    const size_t N = n - m + 1;
+    const size_t grid = (size_t)paddi_tile_width();
+    if (col_lo >= col_hi || col_hi > N || col_lo % grid || (col_hi % grid && col_hi != N))
+        return fail(ctx, PADDI_ERR_INVALID_ARG,
+                    "shard_refine: columns must be [a, b) with a, b multiples of 2048 (b or N)");
+    if (ctx->cap_n < n)
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "shard_refine: run paddi_shard_phase1 first");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->st;
+    const int kernel = refine_kernel_for(ctx, (int)m);
+    const float thr = thr_of(r2, (int)m);
+    CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
+    CK(paddi_launch_compact(d_alive, (int32_t)N, ctx->d_cand, ctx->d_rho, ctx->d_pruned,
+                            ctx->d_rcslot, ctx->d_att, ctx->d_flat, ctx->d_flatcount + 1, (int)m,
+                            r2 > 0.f, st));
+    int launches = 0, nrounds = 0;
+    paddi_status s = refine_rounds(ctx, d_series, (int32_t)N, (int)m, kernel, thr,
+                                   guard_of(ctx, kernel), (int32_t)col_lo, (int32_t)col_hi,
+                                   &launches, &nrounds);
+    if (s != PADDI_OK) return s;
+    CK(cudaMemcpyAsync(&ctx->h_res->n_p1, &ctx->d_att->n_cand_p1, sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const int32_t C = ctx->h_res->n_p1;
+    *n_cand = (uint32_t)C;
+    if ((uint32_t)C > cap)
+        return fail(ctx, PADDI_ERR_INTERNAL_LIMIT,
+                    "shard_refine: " + std::to_string(C) + " candidates, room for " +
+                        std::to_string(cap));
+    if (C > 0) {
+        CK(cudaMemcpyAsync(d_ind, ctx->d_cand, sizeof(int32_t) * C, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(d_rho, ctx->d_rho, sizeof(uint32_t) * C, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(d_pruned, ctx->d_pruned, C, cudaMemcpyDeviceToDevice, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return PADDI_OK;
+}
+
+PADDI_API paddi_status paddi_shard_select(paddi_ctx *ctx, const float *d_series, size_t n,
+                                          uint32_t m, float r2, const int32_t *d_ind,
+                                          const uint32_t *d_rho, const uint8_t *d_pruned,
+                                          uint32_t count, uint32_t top_k, paddi_discord *out,
+                                          uint32_t *n_out, paddi_attempt_log *log)
+{
+    if (!ctx) return PADDI_ERR_INVALID_ARG;
+    if (!d_series || (count && (!d_ind || !d_rho || !d_pruned)) || !out || !n_out ||
+        top_k < 1 || top_k > PADDI_MAX_TOPK || !valid_lengths(n, m, m) || !(r2 >= 0.f))
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "shard_select: invalid argument");
+    const size_t N = n - m + 1;
+    if (count > N || ctx->cap_n < n)
+        return fail(ctx, PADDI_ERR_INVALID_ARG, "shard_select: count or context out of range");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->st;
+    const int kernel = refine_kernel_for(ctx, (int)m);
+    // the merged candidates become this context's candidate arrays
+    CK(cudaMemsetAsync(ctx->d_att, 0, sizeof(PaddiAttemptDev), st));
+    if (count > 0) {
+        CK(cudaMemcpyAsync(ctx->d_cand, d_ind, sizeof(int32_t) * count, cudaMemcpyDeviceToDevice,
+                           st));
+        CK(cudaMemcpyAsync(ctx->d_rho, d_rho, sizeof(uint32_t) * count, cudaMemcpyDeviceToDevice,
+                           st));
+        CK(cudaMemcpyAsync(ctx->d_pruned, d_pruned, count, cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemsetAsync(ctx->d_rcslot, 0xff, sizeof(int32_t) * count, st)); // -1
+    }
+    ctx->h_res->n_p1 = (int32_t)count;
+    CK(cudaMemcpyAsync(&ctx->d_att->n_cand_p1, &ctx->h_res->n_p1, sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(ctx->ev[0], st));
+    CK(cudaEventRecord(ctx->ev[2], st));
+    int launches = 0;
+    bool spec = false;
+    paddi_status s = select_passes(ctx, d_series, n, (int)m, r2, guard_of(ctx, kernel),
+                                   (int)top_k, -1, 0, 0, false, &spec, &launches);
+    if (s != PADDI_OK) return s;
+    AttemptOut a;
+    a.res = *ctx->h_res;
+    a.launches = launches;
+    a.kernel = kernel;
+    CK(cudaEventElapsedTime(&a.ms_select, ctx->ev[2], ctx->ev[3]));
+    a.ms_total = a.ms_select;
+    *n_out = (uint32_t)a.res.n_sel;
+    for (int q = 0; q < a.res.n_sel; ++q) {
+        out[q].ind = a.res.sel_ind[q];
+        out[q].dist = a.res.sel_dist[q];
+    }
+    if (log) fill_log(log, (int)m, std::sqrt(r2), r2, (int)top_k, a, 0.f);
+    return PADDI_OK;
+}
+
+PADDI_API float paddi_merlin_first_r(const paddi_discord *out, uint32_t j, uint32_t minL, float *S)
+{
+    if (j > 0 && !out) return 0.f;
+    return merlin_first_r(out, (int)j, minL, S);
+}
+
+PADDI_API float paddi_merlin_lower(float r, uint32_t j, float S)
+{
+    return merlin_lower(r, (int)j, S);
 }
 
 // ================================================================ test hooks

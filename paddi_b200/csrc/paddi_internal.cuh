@@ -137,11 +137,12 @@ cudaError_t paddi_launch_stats(const float *x, int64_t n, int32_t m, float4 *wst
 
 // Phase 1 at threshold thr = 1 - r^2 / (2m): an exact test (the kernel bounds
 // its own FP32 rounding, no guard band).
+// Only the rows [row_lo, row_hi) are walked (their columns reach anywhere).
 cudaError_t paddi_launch_phase1_dev(const float *x, const float4 *wst, const float *mu,
                                     const double *mu64, uint8_t *alive, int32_t N, int32_t m,
-                                    int32_t R, int32_t max_chunks, float thr,
-                                    int32_t *task_counter, int32_t *walked, int32_t num_sms,
-                                    cudaStream_t st);
+                                    int32_t R, int32_t max_chunks, float thr, int32_t row_lo,
+                                    int32_t row_hi, int32_t *task_counter, int32_t *walked,
+                                    int32_t num_sms, cudaStream_t st);
 
 // prune_flats (r^2 > 0): flat windows with another flat window at least m-1
 // away are dropped (distance 0); flat_span as filled by paddi_launch_stats.
@@ -169,12 +170,14 @@ cudaError_t paddi_launch_fragile_scan_fp32(const float *x, const float4 *wst, co
                                            int32_t *frag_count, int32_t num_sms, cudaStream_t st);
 
 // Exact FP64 correlations of the unpruned candidates of list[0..*list_count)
-// with the fragile windows (k_fragile.cu): prunes and raises rho_max.
+// with the fragile windows in [col_lo, col_hi) (k_fragile.cu): prunes and
+// raises rho_max.
 cudaError_t paddi_launch_fragile(const float *x, const double *mu64, const double *inv64,
                                  const int32_t *cand, const int32_t *list,
                                  const int32_t *list_count, uint8_t *pruned, uint32_t *rho_max,
                                  const int32_t *frag, const int32_t *frag_count, int32_t m,
-                                 float thr, int32_t num_sms, cudaStream_t st);
+                                 float thr, int32_t col_lo, int32_t col_hi, int32_t num_sms,
+                                 cudaStream_t st);
 
 // Tensor-core refine over windows [jb, je) (jb a multiple of the tile width,
 // je too or je = N).  bq / wdq: the per-length tile data of
