@@ -116,6 +116,43 @@ def ref():
     return _REF
 
 
+def refgpu():
+    """The reference's FP32 GPU kernels (src/PD3_kernels.cuh, src/preprocessing.cuh)
+    behind ref_gpu.cu, or None when the prebuilt library is absent."""
+    p = os.path.join(HERE, "_ref", "libpaddi_refgpu.so")
+    if not os.path.exists(p):
+        if has_ref_src():
+            build()
+        else:
+            return None
+    G = C.CDLL(p)
+    f32p = np.ctypeslib.ndpointer(np.float32, flags="C")
+    G.refgpu_palmad.argtypes = [f32p, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                C.POINTER(Discord), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    G.refgpu_palmad.restype = C.c_int32
+    return G
+
+
+def refgpu_palmad(x, minL, maxL, max_attempts, iter_cap=200):
+    """PALMAD with the reference's own FP32 GPU kernels and MERLIN schedule on
+    the current CUDA device, up to the first length boundary after
+    max_attempts attempts.  Returns (completed lengths' discords, attempts,
+    device ms of those attempts)."""
+    G = refgpu()
+    if G is None:
+        return None
+    x = _f32(x)
+    L = maxL - minL + 1
+    out = (Discord * L)()
+    na = C.c_int32(0)
+    ms = C.c_double(0.0)
+    done = G.refgpu_palmad(x, len(x), minL, maxL, iter_cap, max_attempts, out, C.byref(na),
+                           C.byref(ms))
+    if done < 0:
+        raise RuntimeError(f"reference GPU path: CUDA error {-done}")
+    return [(out[i].ind, out[i].dist) for i in range(done)], na.value, ms.value
+
+
 def _f32(x):
     return np.ascontiguousarray(x, dtype=np.float32)
 
