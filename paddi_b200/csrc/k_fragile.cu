@@ -7,9 +7,10 @@
 // g_j that grows with |x_j - s| / |x_j - mu_j| for the shift s of j's tile
 // (window_bound in paddi_internal.cuh).  Windows whose bound exceeds the
 // guard band -- near-flat windows far from their tile's level, series with a
-// large offset and small local variance -- are "fragile": the refine skips
-// them, and this kernel, run after the refine's last round, evaluates them in
-// FP64 against every candidate still unpruned:
+// large offset and small local variance -- are "fragile": the refine uses
+// their correlations only lowered by their own bound (to prune) and keeps no
+// upper estimate of them, and this kernel, run after the refine's last round,
+// evaluates them in FP64 against every candidate still unpruned:
 //     rho = sum_k (x_c+k - mu_c)(x_f+k - mu_f) inv_c inv_f,
 // both windows centred on their own FP64 means, so the error is ~1e-14 of
 // the result whatever the offset.  A correlation above thr + 1e-7 prunes the

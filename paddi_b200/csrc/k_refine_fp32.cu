@@ -26,11 +26,13 @@
 // Rounding: the dot products are summed in two levels (blocks of 64 terms),
 // so a correlation with window j is within g_j = window_bound(E, A_j) of the
 // exact one, A_j the amplification |x_j - sh| / |x_j - mu_j| of the chunk's
-// shift.  Windows with g_j above gcap are fragile: their inverse norm is
-// replaced by NaN (every maximum skips them) and they are evaluated in FP64
-// by the fragile pass.  The chunk's largest other g_j, G, is subtracted from
-// its correlations for the prune test and added back to the kept maxima, so
-// they are the middle of an interval of half-width at most gcap.  Chunks start
+// shift.  Windows with g_j above gcap are fragile: their correlations are
+// lowered by their own g_j (a safe lower bound to prune on) and they are
+// evaluated in FP64 by the fragile pass.  The chunk's largest other g_j, G,
+// is subtracted from the other correlations for the prune test, and added
+// back to the kept maxima, so those are the middle of an interval of
+// half-width at most gcap (a fragile window's lowered value never exceeds its
+// true one).  Chunks start
 // at multiples of 256 windows, so the fragile set depends only on the length.
 #include <float.h>
 
@@ -45,6 +47,7 @@ namespace {
 constexpr int RF_THREADS = 256; // 8 warps x 4 candidates
 constexpr int RF_TC = 32;       // candidates per item
 constexpr int RF_TW = 256;      // windows per chunk (32 lanes x 8)
+static_assert(RF_TW == RF_THREADS, "one window of the chunk per thread at staging");
 constexpr int RF_MAXM = 1024;
 
 __device__ __forceinline__ int xpad(int p) { return p + (p >> 5); }
@@ -55,6 +58,7 @@ struct RfSmem {
     float *cinv;  // [RF_TW]
     float *cmu;   // [RF_TW]
     float *cflt;  // [RF_TW]
+    float *cgm;   // [RF_TW]: the bound subtracted from each window's correlations
 };
 
 constexpr int RF_SUMBLK = 64; // two-level sums: terms per partial sum
@@ -74,6 +78,7 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
     S.cinv = S.xs + xpad(RF_TW + mpad + 8) + 4;
     S.cmu = S.cinv + RF_TW;
     S.cflt = S.cmu + RF_TW;
+    S.cgm = S.cflt + RF_TW;
     __shared__ int s_item, s_alive;
     __shared__ float s_gred[RF_THREADS / 32];
     __shared__ int cw[RF_TC], cp[RF_TC];
@@ -141,17 +146,16 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
                 const int g = j0 + p;
                 S.xs[xpad(p)] = (g < N + m - 1 ? x[g] : sh) - sh;
             }
-            float gq = 0.f; // the chunk's largest bound over its non-fragile windows
-            for (int q = threadIdx.x; q < RF_TW; q += RF_THREADS) {
-                const float4 ws = wst[j0 + q]; // zero beyond N
-                const float mq = mu[j0 + q];
-                const float g = paddi::window_bound(ws.z, mq, sh, (float)m, E, 0.f);
-                const bool frag = j0 + q < N && g > gcap;
-                if (!frag) gq = fmaxf(gq, g);
-                S.cinv[q] = frag ? __int_as_float(0x7fffffff) : ws.z;
-                S.cflt[q] = ws.z == 0.f ? 1.f : 0.f; // flat window (or the padded tail)
-                S.cmu[q] = mq;
-            }
+            // one window per thread (RF_TW == RF_THREADS): its bound, fragile or not
+            const int qt = threadIdx.x;
+            const float4 wsq = wst[j0 + qt]; // zero beyond N
+            const float mq = mu[j0 + qt];
+            const float gt = paddi::window_bound(wsq.z, mq, sh, (float)m, E, 0.f);
+            const bool fragt = j0 + qt < N && gt > gcap;
+            S.cinv[qt] = wsq.z;
+            S.cflt[qt] = wsq.z == 0.f ? 1.f : 0.f; // flat window (or the padded tail)
+            S.cmu[qt] = mq;
+            float gq = fragt ? 0.f : gt; // the chunk's largest bound over its non-fragile windows
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) gq = fmaxf(gq, __shfl_xor_sync(0xffffffffu, gq, o));
             if (lane == 0) s_gred[warp] = gq;
@@ -159,6 +163,8 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
             float G = 0.f;
 #pragma unroll
             for (int w2 = 0; w2 < RF_THREADS / 32; ++w2) G = fmaxf(G, s_gred[w2]);
+            S.cgm[qt] = fragt ? gt : G;
+            __syncthreads();
             float acc[4][8], tot[4][8];
 #pragma unroll
             for (int c = 0; c < 4; ++c)
@@ -208,7 +214,7 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
                     const bool ok = (j < j_hi) && (dd >= m - 1);
                     // lower bound of the correlation (NaN for a fragile window)
                     const float rho = fmaf(fmaf(-zs, S.cmu[q] - sh, tot[c][jj]), S.cinv[q],
-                                           fmaf(fc, S.cflt[q], -G));
+                                           fmaf(fc, S.cflt[q], -S.cgm[q]));
                     if (ok) {
                         cmax = fmaxf(cmax, rho);
                         hit[c] |= rho > thr;
@@ -263,7 +269,7 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
     if ((jb % RF_TW) != 0) return cudaErrorInvalidValue; // chunks on the 256-window grid
     const int mpad = (m + 7) & ~7;
     const size_t smem = sizeof(float) * ((size_t)mpad * RF_TC + (RF_TW + mpad + 8) +
-                                         ((RF_TW + mpad + 8) >> 5) + 4 + 3 * RF_TW) + 16;
+                                         ((RF_TW + mpad + 8) >> 5) + 4 + 4 * RF_TW) + 16;
     cudaError_t e = paddi_raise_smem_limit((const void *)k_refine_fp32, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
