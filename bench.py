@@ -47,6 +47,7 @@ LARGE_CPU_POINTS = 1 << 22
 CPU_SAMPLE_N = 1 << 14          # points per CPU sample slice
 CPU_SLICES_PER_THREAD = 2
 CPU_SAMPLE_LENGTHS = 8          # lengths 64..71
+REF_GPU_ATTEMPTS = 8            # attempts of the reference's GPU path timed (~1 s each)
 L2_FLUSH_BYTES = 512 << 20      # > 126 MB L2
 # DRAM bytes (read + write) of one k_refine_umma launch from an ncu capture:
 # the last refine round (windows N/2..N) of an m=300 attempt on this series
@@ -208,6 +209,62 @@ def cpu_reference(x, steps: int, warmup: int, threads: int, minl: int = MIN_L):
                       f"(slices without a flat run), lengths {minl}..{maxl}, "
                       f"{threads} threads taking slices as they free up",
             "s_per_sample": el}
+
+
+def full_length_point(ctx, st, x, disc, args):
+    """Like for like: one attempt of the reference's CPU kernels on the whole
+    series at length minL (one host thread: the reference has no parallel CPU
+    path) at r just below the length's top-1 distance, and the same attempt on
+    the GPU (device time).  The sample above uses short slices, where DRAG
+    prunes less per matrix cell, so its ratio favours the GPU; this one does not."""
+    import torch
+
+    from oracle import oracle as O
+    m = args.minL
+    r = float(np.sqrt(np.float32(disc[0].dist))) * 0.999
+    t = time.perf_counter()
+    att, _, _ = O.ref_attempt(x, m, r)
+    cpu_s = time.perf_counter() - t
+    ctx.pd3(x, m, top_k=1, r=r)  # warm
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    got, _ = ctx.pd3(x, m, top_k=1, r=r)
+    e1.record(st)
+    e1.synchronize()
+    gpu_ms = e0.elapsed_time(e1)
+    return {"what": f"one attempt at m={m} on all {len(x)} points, r^2={r * r:.4f}",
+            "cpu_s": cpu_s, "cores": 1, "gpu_ms": gpu_ms, "ratio": cpu_s * 1e3 / gpu_ms,
+            "cpu_found": att["top_ind"], "gpu_found": got[0].ind if got else -1,
+            "note": "gpu_ms includes the series upload and statistics of the call"}
+
+
+def reference_gpu_point(x, disc, args, plain_log):
+    """The reference's own FP32 GPU kernels (src/PD3_kernels.cuh,
+    src/preprocessing.cuh, built from the reference's headers into oracle/_ref)
+    with its MERLIN schedule, on the same series, for the first lengths until
+    REF_GPU_ATTEMPTS attempts have run; ms per attempt, and the full run
+    estimated from the attempts the plain form's MERLIN schedule takes."""
+    from oracle import oracle as O
+    try:
+        res = O.refgpu_palmad(x, args.minL, args.maxL, max_attempts=REF_GPU_ATTEMPTS)
+    except (OSError, RuntimeError) as e:
+        return {"unavailable": str(e)}
+    if res is None:
+        return {"unavailable": "oracle/_ref/libpaddi_refgpu.so not built"}
+    done, att, ms = res
+    ours = [(d.ind, d.dist) for d in disc[:len(done)]]
+    errs = [abs(a[1] - b[1]) / b[1] for a, b in zip(done, ours) if b[1] > 0]
+    per = ms / max(att, 1)
+    out = {"what": "reference FP32 GPU kernels (phase 1, define, local refine, host union, "
+                   "node refine) with its MERLIN schedule; first lengths only",
+           "lengths": len(done), "attempts": att, "ms_per_attempt": per,
+           "same_discords_on_those_lengths": [a[0] for a in done] == [b[0] for b in ours],
+           "max_rel_dist_err_vs_fp64": max(errs) if errs else None}
+    if plain_log is not None:
+        out["est_ms_per_step"] = per * len(plain_log)
+        out["est_basis"] = f"{len(plain_log)} MERLIN attempts of the plain form"
+    return out
 
 
 def workload(args):
@@ -435,10 +492,38 @@ def run_paddi(args, world, rank, local):
                               "ms_per_step": ms_plain, "attempts": len(lpl),
                               "speedup_of_headline": ms_plain / step_ms,
                               "same_discords": same}
+    # the form the metric names: split-BF16 tensor-core refine with the same r
+    # policy (the headline's AUTO form runs split FP16), one timed run
+    if not args.no_plain_form and args.dist == "auto":
+        _progress(rank, "split-BF16 form")
+        with P.Context(device=local, distance_kernel=P.DIST_SPLIT_BF16, r_policy=rp) as c3:
+            c3.reserve(n, args.maxL)
+            s3 = torch.cuda.ExternalStream(c3.stream)
+            c3.palmad_device(d_x.data_ptr(), n, args.minL, min(args.maxL, args.minL + 8))
+            flush_l2(0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s3)
+            dbf, lbf = c3.palmad_device(d_x.data_ptr(), n, args.minL, args.maxL)
+            e1.record(s3)
+            e1.synchronize()
+            ms_bf = reduce_max(world, e0.elapsed_time(e1))
+        line["bf16_form"] = {"what": "split-BF16 tensor-core refine (three BF16 products), "
+                                     f"{args.r_policy} r", "ms_per_step": ms_bf,
+                             "attempts": len(lbf),
+                             "same_discords": [(q.ind, q.dist) for q in dbf] ==
+                                              [(q.ind, q.dist) for q in disc],
+                             "speedup_over_plain": (line["plain_form"]["ms_per_step"] / ms_bf
+                                                    if "plain_form" in line else None)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         _progress(rank, "CPU baseline")
         cb = cpu_reference(cpu_sample_of(x, args), 1, 0, min(host_threads(), 64), args.minL)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line["cpu_baseline"]["like_for_like"] = False
+        if args.workload == "palmad":
+            line["cpu_baseline"]["full_length"] = full_length_point(ctx, st, x, disc, args)
+            line["reference_gpu"] = reference_gpu_point(x, disc, args, lpl if not
+                                                        args.no_plain_form else None)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -113,7 +113,7 @@ def compare(series_list, minL, maxL, params, margin=1.0, device=0):
     return rows
 
 
-def evaluate(series_list, minL, maxL, device=0):
+def evaluate(series_list, minL, maxL, device=0, model=None):
     """Attempts and seconds per series for the MERLIN, BOUND and LEARNED
     policies (same kernels); checks that the discords are identical.  A
     policy that reaches the attempt cap on a series (plain MERLIN can: its
@@ -123,7 +123,8 @@ def evaluate(series_list, minL, maxL, device=0):
     for x in series_list:
         rec, ref = {}, None
         for name, pol in (("merlin", R_MERLIN), ("bound", R_BOUND), ("learned", R_LEARNED)):
-            with Context(device=device, r_policy=pol) as ctx:
+            kw = {"model": model} if (pol == R_LEARNED and model is not None) else {}
+            with Context(device=device, r_policy=pol, **kw) as ctx:
                 ctx.palmad(x, minL, minL + 2)  # warm
                 t = time.perf_counter()
                 try:
@@ -152,10 +153,20 @@ def main(argv=None):
     ap.add_argument("--tau", type=float, default=0.2)
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--out", default=DEFAULT_MODEL)
+    ap.add_argument("--model", default=None, help="evaluate: model file (default: the bundled one)")
+    ap.add_argument("--json", default=None, help="evaluate: write the per-series rows here")
     a = ap.parse_args(argv)
     series = datagen.training_series(a.series, a.n, a.seed, min_len=a.minL, max_len=a.maxL)
     if a.cmd == "evaluate":
-        rows = evaluate(series, a.minL, a.maxL)
+        model = None
+        if a.model:
+            model = np.load(a.model)["params"].astype(np.float32)
+        rows = evaluate(series, a.minL, a.maxL, model=model)
+        if a.json:
+            import json
+            with open(a.json, "w") as fh:
+                json.dump({"series": a.series, "n": a.n, "minL": a.minL, "maxL": a.maxL,
+                           "seed": a.seed, "model": a.model or DEFAULT_MODEL, "rows": rows}, fh)
         L = a.maxL - a.minL + 1
         ok = [r for r in rows if all(r[p] is not None for p in r)]
         print(f"series {len(rows)}; plain MERLIN reached the attempt cap on "
