@@ -247,16 +247,13 @@ template <> struct E16<true> {
 // minimises the sum of (mu_j - s)^2 / |x_j - mu_j|^2, so the low-variance
 // windows, where the amplification is large, pull it towards their level);
 // the slice's midrange if no window has a norm.  A window with g_j > gcap is
-// "fragile": its a is NaN in the window data, {a, g_j} go to wfrag[j], and it
-// is appended to frag_list (its pairs with the surviving candidates are
-// evaluated in FP64 after the rounds).  The largest g_j of the block's other
-// windows, G, is stored in the padding entry wd[128].x, the block's number of
-// fragile windows in wd[129 + 128].x.  The epilogue subtracts G from every
-// correlation of the tile (a lower bound that is safe to prune on) and adds
-// it back to the maxima it keeps (the middle of the interval, within gcap of
-// every true value); in a block with fragile windows it takes the per-window
-// path, where a fragile window's correlation is lowered by its own g_j (still a
-// safe lower bound, so the window still prunes the candidates it is close to).
+// "fragile": its a is NaN
+// (the epilogue's maxima skip it) and it is appended to frag_list, whose
+// pairs are evaluated in FP64 later.  The largest g_j of the block's other
+// windows, G, is stored in the padding entry wd[128].x: the epilogue
+// subtracts it from every correlation of the tile (a lower bound that is safe
+// to prune on) and adds it back to the maxima it keeps (the middle of the
+// interval, within gcap of every true value).
 constexpr int TP_THREADS = 256;
 
 template <bool BF>
@@ -264,7 +261,7 @@ __global__ void __launch_bounds__(TP_THREADS)
 k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt, int32_t m,
             const float4 *__restrict__ wst, const float *__restrict__ mu, uint16_t *__restrict__ bq,
             float4 *__restrict__ wdq, float E, float Fu, float gcap, int32_t *frag_list,
-            int32_t *frag_count, float2 *__restrict__ wfrag)
+            int32_t *frag_count)
 {
     using X = E16<BF>;
     __shared__ float red[4][TP_THREADS / 32];
@@ -347,7 +344,6 @@ k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt, int32_t m,
     float *wf = reinterpret_cast<float *>(wdq + (size_t)b * 8 * WD_ROW);
     const float F = Fu * mx, fm = (float)m;
     float gmax = 0.f;
-    int nfrag = 0;
     for (int q = threadIdx.x; q < UM_TW; q += TP_THREADS) {
         const int64_t j = j0 + q; // the padded tail beyond N is zero
         const float iv = wst[j].z, mv = mu[j];
@@ -356,10 +352,6 @@ k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt, int32_t m,
         if (!frag) gmax = fmaxf(gmax, g);
         const int s = q & 7, i = q >> 3, k = i >> 1, slot = i & 1;
         wf[(s * WD_ROW + k) * 4 + slot] = frag ? __int_as_float(0x7fffffff) : iv * dsc;
-        if (frag) {
-            wfrag[j] = make_float2(iv * dsc, g);
-            ++nfrag;
-        }
         wf[(s * WD_ROW + k) * 4 + 2 + slot] = (mv - sh) * iv;
         // fragile windows in index order within each warp (runs stay contiguous)
         const unsigned bal = __ballot_sync(0xffffffffu, frag);
@@ -371,23 +363,13 @@ k_tile_prep(const float *__restrict__ x, int64_t nser, int32_t cnt, int32_t m,
         }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gmax = fmaxf(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
-        nfrag += __shfl_xor_sync(0xffffffffu, nfrag, o);
-    }
-    if (lane == 0) {
-        red[0][w] = gmax;
-        red[1][w] = (float)nfrag;
-    }
+    for (int o = 16; o > 0; o >>= 1) gmax = fmaxf(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
+    if (lane == 0) red[0][w] = gmax;
     __syncthreads();
     if (threadIdx.x == 0) {
-        float G = 0.f, nf = 0.f;
-        for (int k = 0; k < TP_THREADS / 32; ++k) {
-            G = fmaxf(G, red[0][k]);
-            nf += red[1][k];
-        }
-        wf[(0 * WD_ROW + 128) * 4] = G;  // padding entry of shift row 0
-        wf[(1 * WD_ROW + 128) * 4] = nf; // padding entry of shift row 1
+        float G = 0.f;
+        for (int k = 0; k < TP_THREADS / 32; ++k) G = fmaxf(G, red[0][k]);
+        wf[(0 * WD_ROW + 128) * 4] = G; // padding entry of shift row 0
     }
 }
 
@@ -454,7 +436,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
               const uint16_t *__restrict__ bq, const float4 *__restrict__ wdq,
               PaddiAttemptDev *att, uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
               int32_t jb, int32_t je, float thr, int32_t grid_ctas, long long wl,
-              int32_t withhold, const float2 *__restrict__ wfrag)
+              int32_t withhold)
 {
     using X = E16<BF>;
     constexpr int UM_M = MM;
@@ -742,11 +724,8 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 if (!__shfl_sync(0xffffffffu, S.item_dead, 0)) {
                     const uint32_t tb = tmem + ((uint32_t)(32 * g) << 16) +
                                         (uint32_t)(s * UM_N + 128 * hcol);
-                    // per-window path: the range's end, the candidate's exclusion zone,
-                    // a flat candidate, or fragile windows in the tile
                     const bool masked = (j0 + UM_TW > j_hi) ||
-                                        (wc > j0 - m + 1 && wc < j0 + UM_TW + m - 1) || fc != 0.f ||
-                                        wd4[WD_ROW + 128].x != 0.f;
+                                        (wc > j0 - m + 1 && wc < j0 + UM_TW + m - 1) || fc != 0.f;
                     const float4 *wrow = wd4 + bsh * WD_ROW + 64 * hcol;
                     // the tile's rounding bound (tile prep): correlations are lowered
                     // by it for the prune test and raised back for the kept maxima
@@ -774,13 +753,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                                 const float4 wv = wrow[(32 * cb + i) >> 1];
                                 const float wa = (i & 1) ? wv.y : wv.x;
                                 const float wb = (i & 1) ? wv.w : wv.z;
-                                float rho;
-                                if (isnan(wa)) { // fragile: lowered by its own bound
-                                    const float2 fr = wfrag[j];
-                                    rho = fmaf(__uint_as_float(r[i]), fr.x, fmaf(-zsc, wb, -fr.y));
-                                } else {
-                                    rho = fmaf(__uint_as_float(r[i]), wa, fmaf(-zsc, wb, -Gt));
-                                }
+                                float rho = fmaf(__uint_as_float(r[i]), wa, fmaf(-zsc, wb, -Gt));
                                 if (fc != 0.f && wa == 0.f) rho += 1.f; // two flat windows
                                 const int dd = wc > j ? wc - j : j - wc;
                                 if (j < j_hi && dd >= m - 1) tm[i & 3] = fmaxf(tm[i & 3], rho);
@@ -936,7 +909,7 @@ PaddiBound paddi_bound_tc(int m, bool bf16)
 cudaError_t paddi_launch_tile_prep(bool bf16, const float *x, int64_t n, int32_t m,
                                    const float4 *wst, const float *mu, uint16_t *bq, float4 *wdq,
                                    float gcap, int32_t *frag_list, int32_t *frag_count,
-                                   float2 *wfrag, cudaStream_t st)
+                                   cudaStream_t st)
 {
     const int kp = kpad_of(m);
     if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
@@ -945,10 +918,10 @@ cudaError_t paddi_launch_tile_prep(bool bf16, const float *x, int64_t n, int32_t
     const PaddiBound B = paddi_bound_tc(m, bf16);
     if (bf16)
         k_tile_prep<true><<<grid, TP_THREADS, 0, st>>>(x, n, slice_cnt(kp), m, wst, mu, bq, wdq,
-                                                       B.E, B.F, gcap, frag_list, frag_count, wfrag);
+                                                       B.E, B.F, gcap, frag_list, frag_count);
     else
         k_tile_prep<false><<<grid, TP_THREADS, 0, st>>>(x, n, slice_cnt(kp), m, wst, mu, bq, wdq,
-                                                        B.E, B.F, gcap, frag_list, frag_count, wfrag);
+                                                        B.E, B.F, gcap, frag_list, frag_count);
     return cudaGetLastError();
 }
 
@@ -958,7 +931,7 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                                      const float4 *wdq, PaddiAttemptDev *att, uint32_t *rho_max,
                                      uint8_t *pruned, int32_t N, int32_t m, int32_t jb, int32_t je,
                                      float thr_prune, int32_t num_sms, cudaStream_t st,
-                                     long long wait_cycles, int32_t withhold, const float2 *wfrag)
+                                     long long wait_cycles, int32_t withhold)
 {
     const int kp = kpad_of(m);
     if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
@@ -970,7 +943,7 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
     void (*kern)(const float *, const float4 *, const float *, const int32_t *, const int32_t *,
                  const int32_t *, const uint16_t *, const float4 *, PaddiAttemptDev *, uint32_t *,
                  uint8_t *, int32_t, int32_t, int32_t, int32_t, float, int32_t, long long,
-                 int32_t, const float2 *);
+                 int32_t);
     if (MM == 128) kern = bf16 ? k_refine_umma<true, 128> : k_refine_umma<false, 128>;
     else kern = bf16 ? k_refine_umma<true, 64> : k_refine_umma<false, 64>;
     cudaError_t e = paddi_raise_smem_limit((const void *)kern, smem);
@@ -978,7 +951,6 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
     const int grid = num_sms;
     kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, bq, wdq, att, rho_max,
                                          pruned, N, m, jb, je, thr_prune, grid,
-                                         wait_cycles > 0 ? wait_cycles : 4000000000ll, withhold,
-                                         wfrag);
+                                         wait_cycles > 0 ? wait_cycles : 4000000000ll, withhold);
     return cudaGetLastError();
 }

@@ -96,7 +96,6 @@ struct paddi_ctx {
     PaddiAttemptResult *d_res = nullptr;
     int32_t *d_flatcount = nullptr; // {flat windows, flat span (2), fragile windows}
     int32_t *d_frag = nullptr;      // fragile windows of the current length
-    float2 *d_wfrag = nullptr;      // per fragile window: its a and rounding bound (tensor cores)
     PaddiAttemptResult *h_res = nullptr;
     bool umma_ok = false;
     // test hooks (paddi_debug_set): fail the k-th next device allocation; the
@@ -168,7 +167,6 @@ void free_buffers(paddi_ctx *ctx)
     dfree(ctx->d_list[0]);
     dfree(ctx->d_list[1]);
     dfree(ctx->d_frag);
-    dfree(ctx->d_wfrag);
     dfree(ctx->d_bq);
     dfree(ctx->d_wdq);
     dfree(ctx->d_pc);
@@ -200,7 +198,6 @@ paddi_status ensure_capacity(paddi_ctx *ctx, size_t n)
     CK(dmalloc(ctx, &ctx->d_list[0], sizeof(int32_t) * W));
     CK(dmalloc(ctx, &ctx->d_list[1], sizeof(int32_t) * W));
     CK(dmalloc(ctx, &ctx->d_frag, sizeof(int32_t) * W));
-    CK(dmalloc(ctx, &ctx->d_wfrag, sizeof(float2) * W));
     if (ctx->umma_ok) {
         const int64_t blocks = paddi_tile_blocks((int64_t)n);
         CK(dmalloc(ctx, &ctx->d_bq, sizeof(uint16_t) * (size_t)(blocks * paddi_tile_block_elems_max())));
@@ -256,7 +253,7 @@ paddi_status run_stats(paddi_ctx *ctx, const float *x, size_t n, int m, bool til
     if (tiles && kernel != PADDI_DIST_FP32)
         CK(paddi_launch_tile_prep(kernel == PADDI_DIST_SPLIT_BF16, x, (int64_t)n, m, ctx->d_wst,
                                   ctx->d_mu, ctx->d_bq, ctx->d_wdq, guard_of(ctx, kernel),
-                                  ctx->d_frag, ctx->d_flatcount + 3, ctx->d_wfrag, ctx->st));
+                                  ctx->d_frag, ctx->d_flatcount + 3, ctx->st));
     else if (tiles)
         CK(paddi_launch_fragile_scan_fp32(x, ctx->d_wst, ctx->d_mu, (int32_t)(n - m + 1), m,
                                           guard_of(ctx, kernel), ctx->d_frag,
@@ -322,7 +319,7 @@ paddi_status refine_rounds(paddi_ctx *ctx, const float *x, int32_t N, int m, int
                                         &ctx->d_att->list_count[a], ctx->d_bq, ctx->d_wdq,
                                         ctx->d_att, ctx->d_rho, ctx->d_pruned, N, m, jb, je,
                                         thr, ctx->num_sms, st, ctx->wait_cycles,
-                                        ctx->withhold, ctx->d_wfrag));
+                                        ctx->withhold));
         else
             CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
                                         &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,

@@ -191,8 +191,7 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                                      const float4 *wdq, PaddiAttemptDev *att, uint32_t *rho_max,
                                      uint8_t *pruned, int32_t N, int32_t m, int32_t jb, int32_t je,
                                      float thr_prune, int32_t num_sms, cudaStream_t st,
-                                     long long wait_cycles, int32_t withhold,
-                                     const float2 *wfrag);
+                                     long long wait_cycles = 0, int32_t withhold = 0);
 
 // Per-length tile data of the tensor-core refine: for every block of
 // paddi_tile_width() windows, the split 16-bit series slice (bq, at most
@@ -203,11 +202,11 @@ int64_t paddi_tile_blocks(int64_t N);
 int64_t paddi_tile_block_elems_max();
 int64_t paddi_tile_wd_entries();
 // Fragile windows (bound above gcap) are appended to frag_list (frag_count
-// zeroed by the caller) and get {a, bound} in wfrag[window].
+// zeroed by the caller).
 cudaError_t paddi_launch_tile_prep(bool bf16, const float *x, int64_t n, int32_t m,
                                    const float4 *wst, const float *mu, uint16_t *bq, float4 *wdq,
                                    float gcap, int32_t *frag_list, int32_t *frag_count,
-                                   float2 *wfrag, cudaStream_t st);
+                                   cudaStream_t st);
 
 cudaError_t paddi_launch_list_init(const PaddiAttemptDev *att, int32_t *list, int32_t *count,
                                    cudaStream_t st);
