@@ -17,7 +17,12 @@
 //                          - (terms of [w, w+m) not in [w', w'+m+1)),
 // |delta| + |delta + 1| FMA per window instead of m; a slide is taken while
 // that is at most m/4 (and |delta| <= 32).  The centred product is
-//     cov(w, j) = G[j] - m (mu_w - s) (mu_j - s).
+//     cov(w, j) = G[j] - A (mu_j - s),   A = sum_{k<m} (x[w+k] - s),
+// with A summed from the series in FP64 at every launch: writing it as
+// m (mu_w - s) would carry the rounding of the FP64 mean, times |mu_j - s|
+// (series levels far apart), into every correlation -- about 1e-10 relative
+// on a random walk, enough to round a reported distance to the neighbouring
+// float.
 // The shift s is w's mean at the length G was built for, so the shifted
 // values stay of the order of the local range of the series; G is rebuilt
 // with direct dot products after 64 slides, when the window moves further,
@@ -160,9 +165,11 @@ k_guide_stream(const float *__restrict__ x, const double *__restrict__ mu64,
     const double s = g->s;
     const double *Gin = gcur ? G1 : G0;
     double *Gout = gcur ? G0 : G1; // slide only
-    const double mw = mu64[w], iw = inv64[w];
+    const double iw = inv64[w];
     const int fw = flat[w];
-    const double cw = (double)m * (mw - s); // cov = G[j] - cw (mu_j - s)
+    double cw = 0.0; // A: cov = G[j] - A (mu_j - s)
+    for (int k = t; k < m; k += GD_THREADS) cw += (double)x[w + k] - s;
+    cw = block_sum(cw, redm);
     double best = INFINITY;
 
     // ---- the slide's terms: [w, w+m) against the old [gw, gw+gm).  The two
@@ -269,9 +276,13 @@ k_guide_build(const float *__restrict__ x, const double *__restrict__ mu64,
     const double s = mu64[w];
     const double iw = inv64[w];
     const int fw = flat[w];
-    const double cw = 0.0; // s is w's own mean: cov = G[j] exactly
+    double cw = 0.0; // A: s is w's FP64 mean, so A is only its rounding residue
+    for (int k = t; k < m; k += GD_THREADS) {
+        a[k] = (double)x[w + k] - s;
+        cw += a[k];
+    }
+    cw = block_sum(cw, redm);
     double best = INFINITY;
-    for (int k = t; k < m; k += GD_THREADS) a[k] = (double)x[w + k] - s;
     const int nblk = (N + GD_SPAN - 1) / GD_SPAN;
     for (;;) {
         __syncthreads(); // a[] staged; xs free for the next block

@@ -63,6 +63,7 @@ constexpr int P1_THREADS = 32;                // one warp per task
 constexpr int P1_GPT = 4;                     // diagonal pairs per thread
 constexpr int P1_H = P1_THREADS * P1_GPT;     // partner offset (128)
 constexpr int P1_D = 2 * P1_H;                // diagonals per chunk
+static_assert(P1_GPT == 4, "the walk's ring and row maximum are written for 4 pairs");
 constexpr int P1_MAXM = 1024;
 constexpr int P1_SUMBLK = 64;                 // start dot products: terms per partial sum
 constexpr float kU = 5.9604645e-8f;           // unit roundoff of FP32 (2^-24)
@@ -131,7 +132,6 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
         const float4 rd = S.rowdg[s];
         const float2 rt = S.rowt[s];
         const float2 rix = make_float2(rd.x, rd.y), riy = make_float2(rd.z, rd.w);
-        float rmax = -INFINITY;
 #pragma unroll
         for (int k = 0; k < P1_GPT; ++k) {
             const int sl = (u + k) & 3;
@@ -142,11 +142,13 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
                 if (s >= rows || q + P1_H >= lim) vv.y = -INFINITY;
             }
             v[k] = vv;
-            rmax = fmax3(rmax, vv.x, vv.y);
             const float2 cx = make_float2(rxy[sl].x, rxy[sl].y);
             const float2 cy = make_float2(rxy[sl].z, rxy[sl].w);
             cov[k] = __ffma2_rn(rix, cy, __ffma2_rn(cx, riy, cov[k]));
         }
+        // the row's maximum as a tree of depth 2, off the walk's dependency chain
+        const float rmax = fmax3(fmax3(v[0].x, v[0].y, v[1].x), fmax3(v[1].y, v[2].x, v[2].y),
+                                 fmaxf(v[3].x, v[3].y));
         if (__ballot_sync(0xffffffffu, rmax > 0.f) && lane == 0) S.rowflag[s] = 1;
     };
     // the column in ring slot sl leaves: flag it, load column q + 4 into the slot

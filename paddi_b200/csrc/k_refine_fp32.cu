@@ -67,8 +67,9 @@ __global__ void __launch_bounds__(RF_THREADS)
 k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
               const float *__restrict__ mu, const int32_t *__restrict__ cand,
               const int32_t *__restrict__ list, const int32_t *__restrict__ list_count,
-              PaddiAttemptDev *att, uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-              int32_t jb, int32_t je, float thr, int32_t grid_ctas, float E, float gcap)
+              PaddiAttemptDev *att, int32_t *work, uint32_t *rho_max, uint8_t *pruned, int32_t N,
+              int32_t m, int32_t jb, int32_t je, float thr, int32_t grid_ctas, float E,
+              float gcap)
 {
     extern __shared__ __align__(16) unsigned char rf_smem[];
     const int mpad = (m + 7) & ~7;
@@ -97,7 +98,7 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&att->work_next, 1);
+        if (threadIdx.x == 0) s_item = atomicAdd(work, 1);
         __syncthreads();
         const int item = s_item;
         if (item >= total) break;
@@ -261,9 +262,9 @@ k_refine_fp32(const float *__restrict__ x, const float4 *__restrict__ wst,
 cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const float *mu,
                                      const int32_t *cand, const int32_t *list,
                                      const int32_t *list_count, PaddiAttemptDev *att,
-                                     uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     int32_t jb, int32_t je, float thr, float gcap,
-                                     int32_t num_sms, cudaStream_t st)
+                                     int32_t *work, uint32_t *rho_max, uint8_t *pruned,
+                                     int32_t N, int32_t m, int32_t jb, int32_t je, float thr,
+                                     float gcap, int32_t num_sms, cudaStream_t st)
 {
     if (m > RF_MAXM) return cudaErrorInvalidValue;
     if ((jb % RF_TW) != 0) return cudaErrorInvalidValue; // chunks on the 256-window grid
@@ -277,8 +278,8 @@ cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const fl
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int grid = num_sms * per_sm;
-    k_refine_fp32<<<grid, RF_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, att, rho_max,
-                                                  pruned, N, m, jb, je, thr, grid,
+    k_refine_fp32<<<grid, RF_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, att, work,
+                                                  rho_max, pruned, N, m, jb, je, thr, grid,
                                                   paddi_bound_fp32(m).E, gcap);
     return cudaGetLastError();
 }

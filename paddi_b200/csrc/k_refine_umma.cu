@@ -434,8 +434,8 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
               const float *__restrict__ mu, const int32_t *__restrict__ cand,
               const int32_t *__restrict__ list, const int32_t *__restrict__ list_count,
               const uint16_t *__restrict__ bq, const float4 *__restrict__ wdq,
-              PaddiAttemptDev *att, uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-              int32_t jb, int32_t je, float thr, int32_t grid_ctas, long long wl,
+              PaddiAttemptDev *att, int32_t *work, uint32_t *rho_max, uint8_t *pruned, int32_t N,
+              int32_t m, int32_t jb, int32_t je, float thr, int32_t grid_ctas, long long wl,
               int32_t withhold)
 {
     using X = E16<BF>;
@@ -496,7 +496,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
     const float4 *wd4 = reinterpret_cast<const float4 *>(um_smem + L.wd);
 
     for (;;) {
-        if (threadIdx.x == 0) S.item = atomicAdd(&att->work_next, 1);
+        if (threadIdx.x == 0) S.item = atomicAdd(work, 1);
         __syncthreads();
         const int item = S.item;
         if (item >= total || S.abort) break;
@@ -928,10 +928,10 @@ cudaError_t paddi_launch_tile_prep(bool bf16, const float *x, int64_t n, int32_t
 cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *wst,
                                      const float *mu, const int32_t *cand, const int32_t *list,
                                      const int32_t *list_count, const uint16_t *bq,
-                                     const float4 *wdq, PaddiAttemptDev *att, uint32_t *rho_max,
-                                     uint8_t *pruned, int32_t N, int32_t m, int32_t jb, int32_t je,
-                                     float thr_prune, int32_t num_sms, cudaStream_t st,
-                                     long long wait_cycles, int32_t withhold)
+                                     const float4 *wdq, PaddiAttemptDev *att, int32_t *work,
+                                     uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
+                                     int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
+                                     cudaStream_t st, long long wait_cycles, int32_t withhold)
 {
     const int kp = kpad_of(m);
     if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
@@ -941,16 +941,16 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
     // request at least half the SM's shared memory so one CTA owns the 512 TMEM columns
     const size_t smem = L.bytes < 120 * 1024 ? 120 * 1024 : L.bytes;
     void (*kern)(const float *, const float4 *, const float *, const int32_t *, const int32_t *,
-                 const int32_t *, const uint16_t *, const float4 *, PaddiAttemptDev *, uint32_t *,
-                 uint8_t *, int32_t, int32_t, int32_t, int32_t, float, int32_t, long long,
-                 int32_t);
+                 const int32_t *, const uint16_t *, const float4 *, PaddiAttemptDev *, int32_t *,
+                 uint32_t *, uint8_t *, int32_t, int32_t, int32_t, int32_t, float, int32_t,
+                 long long, int32_t);
     if (MM == 128) kern = bf16 ? k_refine_umma<true, 128> : k_refine_umma<false, 128>;
     else kern = bf16 ? k_refine_umma<true, 64> : k_refine_umma<false, 64>;
     cudaError_t e = paddi_raise_smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     const int grid = num_sms;
-    kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, bq, wdq, att, rho_max,
-                                         pruned, N, m, jb, je, thr_prune, grid,
+    kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, bq, wdq, att, work,
+                                         rho_max, pruned, N, m, jb, je, thr_prune, grid,
                                          wait_cycles > 0 ? wait_cycles : 4000000000ll, withhold);
     return cudaGetLastError();
 }

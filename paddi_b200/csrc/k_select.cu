@@ -117,7 +117,8 @@ __global__ void k_list_init(const PaddiAttemptDev *att, int32_t *list, int32_t *
 }
 
 // Keeps the not-yet-pruned entries of a candidate list (order within a
-// block preserved), so the next refine round works on dense tiles.
+// block preserved), so the next refine round works on dense tiles.  out_count
+// is zero on entry (every attempt starts from a zeroed PaddiAttemptDev).
 __global__ void __launch_bounds__(CP_THREADS)
 k_list_compact(const int32_t *__restrict__ in, const int32_t *__restrict__ in_count,
                const uint8_t *__restrict__ pruned, int32_t *out, int32_t *out_count)
@@ -568,8 +569,6 @@ cudaError_t paddi_launch_list_compact(const int32_t *in, const int32_t *in_count
                                       const uint8_t *pruned, int32_t *out, int32_t *out_count,
                                       cudaStream_t st)
 {
-    cudaError_t e = cudaMemsetAsync(out_count, 0, sizeof(int32_t), st);
-    if (e != cudaSuccess) return e;
     k_list_compact<<<64, CP_THREADS, 0, st>>>(in, in_count, pruned, out, out_count);
     return cudaGetLastError();
 }

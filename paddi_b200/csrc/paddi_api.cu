@@ -305,45 +305,47 @@ paddi_status refine_rounds(paddi_ctx *ctx, const float *x, int32_t N, int m, int
                                    : col_lo + (int)((int64_t)range >> kShifts[rd]) / tw * tw;
         if (je > col_hi) je = col_hi;
         if (je < jb) je = jb;
+        // round rd: list d_list[rd & 1] of list_count[rd] entries, work counter
+        // work_rd[rd]; the compaction after it writes list_count[rd + 1].  All
+        // are zero from the attempt's reset, so no launch clears them.
         const int a = rd & 1, b = a ^ 1;
+        int32_t *cnt = &ctx->d_att->list_count[rd];
         if (ctx->trace) {
             CK(cudaEventRecord(ctx->tev[rd], st));
-            CK(cudaMemcpyAsync(ctx->d_trace + rd, &ctx->d_att->list_count[a], sizeof(int32_t),
+            CK(cudaMemcpyAsync(ctx->d_trace + rd, cnt, sizeof(int32_t),
                                cudaMemcpyDeviceToDevice, st));
         }
-        CK(cudaMemsetAsync(&ctx->d_att->work_next, 0, sizeof(int32_t), st));
         CK(cudaEventRecord(ctx->rev[2 * rd], st));
         if (umma)
             CK(paddi_launch_refine_umma(kernel == PADDI_DIST_SPLIT_BF16, x, ctx->d_wst, ctx->d_mu,
-                                        ctx->d_cand, ctx->d_list[a],
-                                        &ctx->d_att->list_count[a], ctx->d_bq, ctx->d_wdq,
-                                        ctx->d_att, ctx->d_rho, ctx->d_pruned, N, m, jb, je,
-                                        thr, ctx->num_sms, st, ctx->wait_cycles,
-                                        ctx->withhold));
+                                        ctx->d_cand, ctx->d_list[a], cnt, ctx->d_bq,
+                                        ctx->d_wdq, ctx->d_att, &ctx->d_att->work_rd[rd],
+                                        ctx->d_rho, ctx->d_pruned, N, m, jb, je, thr,
+                                        ctx->num_sms, st, ctx->wait_cycles, ctx->withhold));
         else
             CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
-                                        &ctx->d_att->list_count[a], ctx->d_att, ctx->d_rho,
+                                        cnt, ctx->d_att, &ctx->d_att->work_rd[rd], ctx->d_rho,
                                         ctx->d_pruned, N, m, jb, je, thr, guard, ctx->num_sms,
                                         st));
         CK(cudaEventRecord(ctx->rev[2 * rd + 1], st));
         ++*launches;
         if (rd + 1 < nrounds) {
-            CK(paddi_launch_list_compact(ctx->d_list[a], &ctx->d_att->list_count[a],
-                                         ctx->d_pruned, ctx->d_list[b],
-                                         &ctx->d_att->list_count[b], st));
+            CK(paddi_launch_list_compact(ctx->d_list[a], cnt, ctx->d_pruned, ctx->d_list[b],
+                                         cnt + 1, st));
             ++*launches;
         }
         jb = je;
     }
     // the fragile windows (skipped by the refine: their rounding bound exceeds
-    // the guard band) against the candidates the rounds left, in FP64
-    const int a = (nrounds - 1) & 1, b = a ^ 1;
-    CK(paddi_launch_list_compact(ctx->d_list[a], &ctx->d_att->list_count[a], ctx->d_pruned,
-                                 ctx->d_list[b], &ctx->d_att->list_count[b], st));
-    CK(paddi_launch_fragile(x, ctx->d_mu64, ctx->d_inv64, ctx->d_cand, ctx->d_list[b],
-                            &ctx->d_att->list_count[b], ctx->d_pruned, ctx->d_rho, ctx->d_frag,
-                            ctx->d_flatcount + 3, m, thr, col_lo, col_hi, ctx->num_sms, st));
-    *launches += 2;
+    // the guard band) against the candidates of the last round's list that are
+    // still unpruned, in FP64 (the kernel returns at once when there are none)
+    const int a = (nrounds - 1) & 1;
+    if (ctx->trace) CK(cudaEventRecord(ctx->tev[nrounds], st));
+    CK(paddi_launch_fragile(x, ctx->d_mu64, ctx->d_inv64, ctx->d_cand, ctx->d_list[a],
+                            &ctx->d_att->list_count[nrounds - 1], ctx->d_pruned, ctx->d_rho,
+                            ctx->d_frag, ctx->d_flatcount + 3, m, thr, col_lo, col_hi,
+                            ctx->num_sms, st));
+    *launches += 1;
     *nrounds_out = nrounds;
     return PADDI_OK;
 }
@@ -460,7 +462,7 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
     if (s != PADDI_OK) return s;
     CK(cudaEventRecord(ctx->ev[2], st));
     if (ctx->trace) {
-        CK(cudaEventRecord(ctx->tev[nrounds], st));
+        CK(cudaEventRecord(ctx->tev[nrounds + 1], st));
         CK(cudaMemcpyAsync(ctx->d_trace + 7, &ctx->d_att->p1_walked, sizeof(int32_t),
                            cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(ctx->h_trace64, &ctx->d_att->n_pairs, 2 * sizeof(unsigned long long),
@@ -485,9 +487,11 @@ paddi_status run_attempt(paddi_ctx *ctx, const float *x, size_t n, int m, float 
             CK(cudaEventElapsedTime(&ms, ctx->tev[rd], ctx->tev[rd + 1]));
             line += " " + std::to_string(ctx->h_trace[rd]) + "/" + std::to_string(ms);
         }
-        std::fprintf(stderr, "%s disc=%lld pairs=%llu live=%llu fragile=%d\n", line.c_str(),
+        float fms = 0.f;
+        CK(cudaEventElapsedTime(&fms, ctx->tev[nrounds], ctx->tev[nrounds + 1]));
+        std::fprintf(stderr, "%s disc=%lld pairs=%llu live=%llu fragile=%d/%f\n", line.c_str(),
                      (long long)ctx->h_res->n_disc, ctx->h_trace64[0], ctx->h_trace64[1],
-                     ctx->h_res->n_fragile);
+                     ctx->h_res->n_fragile, fms);
     }
     CK(cudaEventElapsedTime(&out->ms_phase1, ctx->ev[0], ctx->ev[1]));
     CK(cudaEventElapsedTime(&out->ms_refine, ctx->ev[1], ctx->ev[2]));

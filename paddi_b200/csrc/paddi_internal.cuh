@@ -82,12 +82,14 @@ PaddiBound paddi_bound_fp32(int m);
 // Per-attempt device-side state shared by the kernels of one (m, r) attempt.
 struct PaddiAttemptDev {
     int32_t n_cand_p1;      // candidates after phase 1 (compacted list length)
-    int32_t work_next;      // work-item counter of the refine kernel
+    int32_t work_rd[4];     // work-item counters of the refine rounds (one per round)
     int32_t recheck_next;   // work-item counter of the FP64 recheck kernel
     int32_t n_recheck;      // windows queued for the FP64 recheck
     int32_t status;         // nonzero: a kernel hit an internal limit
     int32_t task_next;      // task counter of the phase-1 kernel
-    int32_t list_count[2];  // lengths of the ping-pong candidate lists of the refine rounds
+    int32_t list_count[5];  // candidate-list length entering each refine round (and after
+                            // the last); zero when the attempt starts, so the compactions
+                            // between rounds need no reset
     int32_t p1_walked;      // phase-1 tasks that walked their rows (instrumentation)
     unsigned long long n_pairs; // pairs evaluated by the refine (instrumentation)
     unsigned long long n_live;  // of those, pairs of candidates still unpruned at the tile's start
@@ -159,9 +161,9 @@ cudaError_t paddi_launch_compact(const uint8_t *alive, int32_t N, int32_t *cand,
 cudaError_t paddi_launch_refine_fp32(const float *x, const float4 *wst, const float *mu,
                                      const int32_t *cand, const int32_t *list,
                                      const int32_t *list_count, PaddiAttemptDev *att,
-                                     uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
-                                     int32_t jb, int32_t je, float thr, float gcap,
-                                     int32_t num_sms, cudaStream_t st);
+                                     int32_t *work, uint32_t *rho_max, uint8_t *pruned,
+                                     int32_t N, int32_t m, int32_t jb, int32_t je, float thr,
+                                     float gcap, int32_t num_sms, cudaStream_t st);
 
 // Fragile windows of length m in the FP32 refine's geometry, appended to
 // frag_list (frag_count zeroed by the caller).
@@ -188,8 +190,9 @@ cudaError_t paddi_launch_fragile(const float *x, const double *mu64, const doubl
 cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *wst,
                                      const float *mu, const int32_t *cand, const int32_t *list,
                                      const int32_t *list_count, const uint16_t *bq,
-                                     const float4 *wdq, PaddiAttemptDev *att, uint32_t *rho_max,
-                                     uint8_t *pruned, int32_t N, int32_t m, int32_t jb, int32_t je,
+                                     const float4 *wdq, PaddiAttemptDev *att, int32_t *work,
+                                     uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
+                                     int32_t jb, int32_t je,
                                      float thr_prune, int32_t num_sms, cudaStream_t st,
                                      long long wait_cycles = 0, int32_t withhold = 0);
 

@@ -101,13 +101,14 @@ def pd3_series(n: int = 131072, seed: int = 0, n_anom: int = 4,
 
 
 def palmad_series(n: int = 1 << 21, seed: int = 1, n_anom: int = 16,
-                  min_len: int = 64, max_len: int = 512):
+                  min_len: int = 64, max_len: int = 512,
+                  kinds_cycle=("noise", "flat", "reverse")):
     """Arbitrary-length workload: same generator, ``n_anom`` anomalies with
-    lengths U[min_len, max_len] cycling through noise / flat / reverse."""
+    lengths U[min_len, max_len] cycling through ``kinds_cycle``."""
     rng = np.random.default_rng(seed)
     x = random_walk_sine(n, rng)
     lengths = [int(v) for v in rng.integers(min_len, max_len + 1, n_anom)]
-    kinds = [("noise", "flat", "reverse")[i % 3] for i in range(n_anom)]
+    kinds = [kinds_cycle[i % len(kinds_cycle)] for i in range(n_anom)]
     starts = _non_overlapping_starts(n, lengths, rng, margin=max_len)
     plant_anomalies(x, starts, lengths, kinds, rng)
     return x.astype(np.float32), {"starts": starts, "lengths": lengths,

@@ -113,17 +113,24 @@ def compare(series_list, minL, maxL, params, margin=1.0, device=0):
     return rows
 
 
-def evaluate(series_list, minL, maxL, device=0, model=None):
+def evaluate(series_list, minL, maxL, device=0, model=None, policies=("merlin", "bound", "learned"),
+             margin=1.0):
     """Attempts and seconds per series for the MERLIN, BOUND and LEARNED
     policies (same kernels); checks that the discords are identical.  A
     policy that reaches the attempt cap on a series (plain MERLIN can: its
     decrement S of src/main.cu:230 may vanish) is recorded as None."""
     from . import R_BOUND
+    codes = {"merlin": R_MERLIN, "bound": R_BOUND, "learned": R_LEARNED}
     rows = []
     for x in series_list:
         rec, ref = {}, None
-        for name, pol in (("merlin", R_MERLIN), ("bound", R_BOUND), ("learned", R_LEARNED)):
-            kw = {"model": model} if (pol == R_LEARNED and model is not None) else {}
+        for name in policies:
+            pol = codes[name]
+            kw = {}
+            if pol == R_LEARNED:
+                kw["model_margin"] = margin
+                if model is not None:
+                    kw["model"] = model
             with Context(device=device, r_policy=pol, **kw) as ctx:
                 ctx.palmad(x, minL, minL + 2)  # warm
                 t = time.perf_counter()
@@ -155,23 +162,41 @@ def main(argv=None):
     ap.add_argument("--out", default=DEFAULT_MODEL)
     ap.add_argument("--model", default=None, help="evaluate: model file (default: the bundled one)")
     ap.add_argument("--json", default=None, help="evaluate: write the per-series rows here")
+    ap.add_argument("--policies", default="merlin,bound,learned",
+                    help="evaluate: comma-separated subset of merlin,bound,learned")
+    ap.add_argument("--margin", type=float, default=1.0,
+                    help="evaluate: scale of the model's predicted r^2")
+    ap.add_argument("--first", type=int, default=0,
+                    help="evaluate: only the first this many series (0: all)")
+    ap.add_argument("--save-samples", default=None,
+                    help="train: also write the collected (X, Y) pairs to this .npz")
+    ap.add_argument("--samples", default=None,
+                    help="train: read (X, Y) pairs from this .npz instead of collecting them")
     a = ap.parse_args(argv)
-    series = datagen.training_series(a.series, a.n, a.seed, min_len=a.minL, max_len=a.maxL)
+    if a.cmd == "train" and a.samples:
+        series = []
+    else:
+        series = datagen.training_series(a.series, a.n, a.seed, min_len=a.minL, max_len=a.maxL)
     if a.cmd == "evaluate":
         model = None
         if a.model:
             model = np.load(a.model)["params"].astype(np.float32)
-        rows = evaluate(series, a.minL, a.maxL, model=model)
+        if a.first:
+            series = series[:a.first]
+        pols = tuple(p for p in a.policies.split(",") if p)
+        rows = evaluate(series, a.minL, a.maxL, model=model, policies=pols, margin=a.margin)
         if a.json:
             import json
             with open(a.json, "w") as fh:
-                json.dump({"series": a.series, "n": a.n, "minL": a.minL, "maxL": a.maxL,
-                           "seed": a.seed, "model": a.model or DEFAULT_MODEL, "rows": rows}, fh)
+                json.dump({"series": len(rows), "n": a.n, "minL": a.minL, "maxL": a.maxL,
+                           "seed": a.seed, "model": a.model or DEFAULT_MODEL,
+                           "margin": a.margin, "rows": rows}, fh)
         L = a.maxL - a.minL + 1
         ok = [r for r in rows if all(r[p] is not None for p in r)]
+        capped_m = sum(1 for r in rows if "merlin" in r and r["merlin"] is None)
         print(f"series {len(rows)}; plain MERLIN reached the attempt cap on "
-              f"{sum(1 for r in rows if r['merlin'] is None)}; totals over the other {len(ok)}")
-        for name in ("merlin", "bound", "learned"):
+              f"{capped_m}; totals over the other {len(ok)}")
+        for name in pols:
             att = sum(r[name]["attempts"] for r in ok)
             sec = sum(r[name]["s"] for r in ok)
             same = all(r[name]["same"] for r in ok)
@@ -180,7 +205,15 @@ def main(argv=None):
                   f"same discords {same}  capped {capped}")
         return
     t = time.perf_counter()
-    X, Y, runs = collect(series, a.minL, a.maxL)
+    if a.samples:
+        d = np.load(a.samples)
+        X, Y = d["X"].astype(np.float32), d["Y"].astype(np.float32)
+        runs = [{"skipped": bool(v)} for v in d["skipped"]]
+    else:
+        X, Y, runs = collect(series, a.minL, a.maxL)
+        if a.save_samples:
+            np.savez_compressed(a.save_samples, X=X, Y=Y,
+                                skipped=np.array([bool(r.get("skipped")) for r in runs]))
     t_collect = time.perf_counter() - t
     t = time.perf_counter()
     params, loss = train(X, Y, tau=a.tau, epochs=a.epochs)

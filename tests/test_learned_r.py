@@ -147,3 +147,21 @@ def test_learned_policy_returns_the_same_discords_with_any_model():
         for d, w in zip(got, want):
             assert abs(d.dist - w[1]) <= 1e-5 * abs(w[1])
         assert any(e["r_source"] == 1 for e in log)
+
+
+@pytest.mark.gpu
+def test_trained_model_saves_attempts_on_held_out_series():
+    """What the network gains: on series from a seed not used in training
+    (the held-out evaluation of the training recipe, scaled to fit the test
+    budget: 4 series of 2^18, lengths 64..320), the learned policy needs no
+    more attempts in total than the exact-bound policy alone and fewer than
+    the reference's MERLIN schedule, with identical discords."""
+    from paddi_b200 import learned_r
+    series = datagen.training_series(4, 1 << 18, 97, min_len=64, max_len=320)
+    rows = learned_r.evaluate(series, 64, 320, model=learned_r.load_default())
+    ok = [r for r in rows if all(r[p] is not None for p in r)]
+    assert len(ok) >= 3  # MERLIN may hit its attempt cap on a series (S vanishes)
+    tot = {p: sum(r[p]["attempts"] for r in ok) for p in ("merlin", "bound", "learned")}
+    assert all(r[p]["same"] for r in ok for p in r)
+    assert tot["learned"] <= tot["bound"], tot
+    assert tot["learned"] < tot["merlin"], tot
