@@ -17,15 +17,14 @@
 // candidate (the margin covers the FP32 rounding of thr); every value enters
 // the candidate's kept maximum.
 //
-// Work items: (8 candidates of the list, 64 consecutive entries of the
-// fragile list).  Fragile windows come in runs (tile prep and the FP32 scan
-// append them in index order within each warp), so an item's windows usually
-// span a short stretch of the series: it is staged in shared memory once and
-// each thread evaluates one window against 2 of the 8 candidates (whose
-// centred values also sit in shared memory).  An item whose windows span more
-// than FG_SPAN values reads the series from global memory instead.
+// Work items: (a group of 8 entries of the candidate list, 256 consecutive
+// entries of the fragile list).  The group's centred candidate values sit in
+// shared memory (read as broadcasts, two terms per load); each thread owns
+// one fragile window, reads its values once per 4-candidate half of the group
+// straight from the series (consecutive addresses per thread, so 7 of 8
+// loads hit L1) and keeps 4 FP64 accumulators.  Halves whose candidates are
+// all pruned, and items with no live candidate, are skipped.
 #include <float.h>
-#include <limits.h>
 
 #include "paddi_internal.cuh"
 
@@ -33,12 +32,10 @@ using paddi::f2ord;
 
 namespace {
 
-constexpr int FG_THREADS = 256;
-constexpr int FG_CAND = 8;     // candidates per work item
-constexpr int FG_WIN = 64;     // fragile windows per work item
-constexpr int FG_SPAN = 3072;  // longest staged stretch of the series
+constexpr int FG_THREADS = 256; // fragile windows per item (one per thread)
+constexpr int FG_CAND = 8;      // candidate-list entries per item
+constexpr int FG_HALF = 4;      // accumulators per thread
 constexpr int FG_MAXM = 1024;
-static_assert(FG_THREADS == FG_WIN * FG_CAND / 2, "one window and two candidates per thread");
 
 __global__ void __launch_bounds__(FG_THREADS)
 k_fragile(const float *__restrict__ x, const double *__restrict__ mu64,
@@ -48,99 +45,93 @@ k_fragile(const float *__restrict__ x, const double *__restrict__ mu64,
           const int32_t *__restrict__ frag_count, int32_t m, float thr, int32_t col_lo,
           int32_t col_hi)
 {
-    extern __shared__ __align__(16) double fg_a[]; // [FG_CAND][m]: centred candidates
-    __shared__ float xs[FG_SPAN];                  // the item's stretch of the series
+    // [FG_CAND][mp] centred candidate values, mp = m rounded up to even
+    extern __shared__ __align__(16) double fg_a[];
     __shared__ int cw[FG_CAND], cp[FG_CAND], live[FG_CAND];
-    __shared__ int fw[FG_WIN];
+    __shared__ double civ[FG_CAND];
     __shared__ double best_s[FG_CAND][FG_THREADS / 32];
-    __shared__ int s_any, s_lo, s_hi;
+    __shared__ int s_any;
     const int C = *list_count, F = *frag_count;
     if (C <= 0 || F <= 0) return;
+    const int mp = (m + 1) & ~1;
     const int groups = (C + FG_CAND - 1) / FG_CAND;
-    const int chunks = (F + FG_WIN - 1) / FG_WIN;
+    const int chunks = (F + FG_THREADS - 1) / FG_THREADS;
     const long long total = (long long)groups * chunks;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int wi = t & (FG_WIN - 1);          // this thread's window of the item
-    const int c0 = t / FG_WIN, c1 = c0 + FG_CAND / 2;
     for (long long item = blockIdx.x; item < total; item += gridDim.x) {
         const int grp = (int)(item % groups), chunk = (int)(item / groups);
-        __syncthreads();
-        if (t == 0) {
-            s_any = 0;
-            s_lo = INT_MAX;
-            s_hi = -1;
-        }
+        __syncthreads(); // the previous item's shared data is consumed
+        if (t == 0) s_any = 0;
         __syncthreads();
         if (t < FG_CAND) {
             const int li = grp * FG_CAND + t;
             const int pos = li < C ? list[li] : -1;
+            const int w = pos >= 0 ? cand[pos] : 0;
             cp[t] = pos;
-            cw[t] = pos >= 0 ? cand[pos] : 0;
+            cw[t] = w;
             live[t] = pos >= 0 && !__ldcg(pruned + pos);
+            civ[t] = inv64[w];
             if (live[t]) atomicOr(&s_any, 1);
         }
-        if (t < FG_WIN) {
-            const int fi = chunk * FG_WIN + t;
-            const int f = fi < F ? frag[fi] : -1;
-            fw[t] = (f >= col_lo && f < col_hi) ? f : -1;
-            if (fw[t] >= 0) {
-                atomicMin(&s_lo, f);
-                atomicMax(&s_hi, f);
-            }
+        __syncthreads();
+        if (!s_any) continue;
+        for (int e = t; e < FG_CAND * mp; e += FG_THREADS) {
+            const int c = e / mp, k = e - c * mp;
+            fg_a[e] = (live[c] && k < m) ? (double)x[cw[c] + k] - mu64[cw[c]] : 0.0;
         }
         __syncthreads();
-        if (!s_any || s_hi < 0) continue;
-        const int lo = s_lo, span = s_hi - s_lo + m;
-        const bool staged = span <= FG_SPAN;
-        for (int e = t; e < FG_CAND * m; e += FG_THREADS) {
-            const int c = e / m, k = e - c * m;
-            fg_a[e] = live[c] ? (double)x[cw[c] + k] - mu64[cw[c]] : 0.0;
-        }
-        if (staged)
-            for (int p = t; p < span; p += FG_THREADS) xs[p] = x[lo + p];
-        __syncthreads();
-        double b0 = -INFINITY, b1 = -INFINITY;
-        const int f = fw[wi];
-        if (f >= 0 && (live[c0] || live[c1])) {
+        const int fi = chunk * FG_THREADS + t;
+        const int f = fi < F ? frag[fi] : -1;
+        const bool fok = f >= col_lo && f < col_hi;
+        double b[FG_CAND];
+#pragma unroll
+        for (int c = 0; c < FG_CAND; ++c) b[c] = -INFINITY;
+#pragma unroll
+        for (int h = 0; h < FG_CAND / FG_HALF; ++h) {
+            const int c0 = h * FG_HALF;
+            bool any = false;
+#pragma unroll
+            for (int c = 0; c < FG_HALF; ++c) any |= live[c0 + c] != 0;
+            if (!any || !fok) continue; // any: uniform over the block
             const double mf = mu64[f];
-            const double *a0 = fg_a + c0 * m, *a1 = fg_a + c1 * m;
-            double acc0 = 0.0, acc1 = 0.0;
-            if (staged) {
-                const float *y = xs + (f - lo);
+            const float *y = x + f;
+            const double2 *a2 = reinterpret_cast<const double2 *>(fg_a + c0 * mp);
+            const int mh = mp >> 1;
+            double acc[FG_HALF];
+#pragma unroll
+            for (int c = 0; c < FG_HALF; ++c) acc[c] = 0.0;
 #pragma unroll 4
-                for (int k = 0; k < m; ++k) {
-                    const double v = (double)y[k] - mf;
-                    acc0 = fma(a0[k], v, acc0);
-                    acc1 = fma(a1[k], v, acc1);
-                }
-            } else {
-                const float *y = x + f;
-#pragma unroll 8
-                for (int k = 0; k < m; ++k) {
-                    const double v = (double)__ldg(y + k) - mf;
-                    acc0 = fma(a0[k], v, acc0);
-                    acc1 = fma(a1[k], v, acc1);
+            for (int q = 0; q < mh; ++q) {
+                // terms 2q, 2q+1 (the even padding term has zero candidate values)
+                const double v0 = (double)__ldg(y + 2 * q) - mf;
+                const double v1 = 2 * q + 1 < m ? (double)__ldg(y + 2 * q + 1) - mf : 0.0;
+#pragma unroll
+                for (int c = 0; c < FG_HALF; ++c) {
+                    const double2 av = a2[c * mh + q];
+                    acc[c] = fma(av.y, v1, fma(av.x, v0, acc[c]));
                 }
             }
             const double ivf = inv64[f];
-            const int d0 = cw[c0] > f ? cw[c0] - f : f - cw[c0];
-            const int d1 = cw[c1] > f ? cw[c1] - f : f - cw[c1];
-            if (live[c0] && d0 >= m - 1) b0 = acc0 * inv64[cw[c0]] * ivf;
-            if (live[c1] && d1 >= m - 1) b1 = acc1 * inv64[cw[c1]] * ivf;
-        }
-        // maxima over the item's 64 windows: two warps per candidate pair
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            b0 = fmax(b0, __shfl_xor_sync(0xffffffffu, b0, o));
-            b1 = fmax(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+            for (int c = 0; c < FG_HALF; ++c) {
+                const int ci = c0 + c;
+                const int d = cw[ci] > f ? cw[ci] - f : f - cw[ci];
+                if (live[ci] && d >= m - 1) b[ci] = acc[c] * civ[ci] * ivf;
+            }
         }
-        if (lane == 0) {
-            best_s[c0][warp & 1] = b0;
-            best_s[c1][warp & 1] = b1;
+        // maxima over the item's windows, per candidate
+#pragma unroll
+        for (int c = 0; c < FG_CAND; ++c) {
+            double v = b[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if (lane == 0) best_s[c][warp] = v;
         }
         __syncthreads();
         if (t < FG_CAND && live[t]) {
-            const double v = fmax(best_s[t][0], best_s[t][1]);
+            double v = -INFINITY;
+#pragma unroll
+            for (int q = 0; q < FG_THREADS / 32; ++q) v = fmax(v, best_s[t][q]);
             if (v > -INFINITY) {
                 atomicMax(rho_max + cp[t], f2ord((float)v));
                 if (v > (double)thr + 1e-7) pruned[cp[t]] = 1;
@@ -158,8 +149,8 @@ cudaError_t paddi_launch_fragile(const float *x, const double *mu64, const doubl
                                  float thr, int32_t col_lo, int32_t col_hi, int32_t num_sms,
                                  cudaStream_t st)
 {
-    if (m > FG_MAXM) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(double) * (size_t)FG_CAND * m;
+    if (m > FG_MAXM || m < 3) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(double) * (size_t)FG_CAND * (size_t)((m + 1) & ~1);
     cudaError_t e = paddi_raise_smem_limit((const void *)k_fragile, smem);
     if (e != cudaSuccess) return e;
     k_fragile<<<num_sms * 4, FG_THREADS, smem, st>>>(x, mu64, inv64, cand, list, list_count,

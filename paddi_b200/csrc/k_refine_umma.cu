@@ -62,6 +62,7 @@ constexpr int UM_THREADS = 384;  // 12 warps
 constexpr int UM_TCMAX = 16;     // candidates per tile (M = 128); 8 for M = 64
 constexpr int UM_N = 256;        // windows at stride 8
 constexpr int UM_TW = UM_N * 8;  // windows per tile (one block of the grid)
+constexpr int UM_WAVES = 2;      // work items per CTA and round when candidate tiles are few
 constexpr int UM_KMAX128 = 368;  // largest K' with M = 128 (shared-memory bound)
 constexpr int UM_KMAX64 = 736;   // largest K' with M = 64
 constexpr int ZSCALE = 8;        // zhat scaled by 2^8 before splitting
@@ -409,6 +410,7 @@ struct UmShared {
     int last_full[2], last_wd;
     uint32_t tmem_base;
     int item, abort, tok;
+    int built_tile; // candidate tile whose operand sits in A (-1: none)
     volatile int item_dead;
     int tile_live; // live candidates at the start of the current tile (instrumentation)
     volatile int vb[2], vw;
@@ -462,6 +464,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
         mbar_init(&S.wd_empty, EPI_WARPS);
         mbar_init(&S.drain, 1);
         S.abort = 0;
+        S.built_tile = -1;
         S.last_full[0] = S.last_full[1] = S.last_wd = -1;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -481,8 +484,9 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
 
     const int range = je - jb;
     const int tiles = (C + UM_TC - 1) / UM_TC;
-    int splits = (2 * grid_ctas + tiles - 1) / tiles;
-    splits = max(1, min(splits, max(1, range / (2 * UM_TW))));
+    // at most UM_WAVES items per CTA when the candidate tiles are few, items of
+    // at least one 2048-window block
+    const int splits = max(1, min(range / UM_TW, (UM_WAVES * grid_ctas) / tiles));
     const int span = (((range + splits - 1) / splits) + UM_TW - 1) / UM_TW * UM_TW;
     const int total = tiles * splits;
     const uint32_t idesc = idesc_f16(X::fmt, UM_M, UM_N);
@@ -544,8 +548,11 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
                 S.last_full[0] = (int)ph.full[0];
             }
         }
-        // ---- candidate operand: 16 x (hi, lo) rows of scaled zhat, then 8 shifted copies
-        {
+        // ---- candidate operand: 16 x (hi, lo) rows of scaled zhat, then 8 shifted
+        //      copies; kept from the CTA's previous item when that had the same
+        //      candidate tile (a candidate pruned since then only costs its rows'
+        //      work: its results no longer matter)
+        if (S.built_tile != tile) {
             // scratch rows of 32-bit words: 4 zero words (8 elements) of front
             // padding, then zhat[0..kp); stride ksw words with ksw % 32 == 8, so
             // the four candidates a warp reads sit in disjoint bank ranges
@@ -614,6 +621,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
             }
             fence_proxy_async_smem(); // A for the tensor core; scratch for the bulk copies
             __syncthreads();
+            if (threadIdx.x == 0) S.built_tile = tile; // read after the next item's barrier
         }
 
         // ================================================================ roles

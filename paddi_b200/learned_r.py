@@ -11,11 +11,14 @@ Training data are the method's own logs: plain MERLIN PALMAD runs
 from ``datagen.training_series``.  A wrong prediction never changes the
 discords, only the number of attempts.
 
-Recipe (GPU):
-    python -m paddi_b200.learned_r train --series 64 --n 131072 --minL 64 --maxL 512
-writes paddi_b200/models/r_mlp.npz; ``load_default`` reads it.  Evaluation on
-held-out series (another seed), all three r policies:
-    python -m paddi_b200.learned_r evaluate --series 8 --n 1048576 --minL 64 --maxL 1024 --seed 97
+Recipe of the bundled model (GPU; collecting the logs of 512 MERLIN runs on
+series of 2^18 points at lengths 64..1024 takes ~14 minutes on a B200, the
+training a few seconds):
+    python -m paddi_b200.learned_r train --series 512 --n 262144 --minL 64 --maxL 1024 --seed 31 --tau 0.1
+writes paddi_b200/models/r_mlp.npz; ``load_default`` reads it (``--save-samples``
+keeps the collected pairs, ``--samples`` trains from them again).  Evaluation
+on held-out series (another seed), all three r policies:
+    python -m paddi_b200.learned_r evaluate --series 64 --n 1048576 --minL 64 --maxL 1024 --seed 97
 """
 from __future__ import annotations
 
@@ -157,7 +160,7 @@ def main(argv=None):
     ap.add_argument("--minL", type=int, default=64)
     ap.add_argument("--maxL", type=int, default=512)
     ap.add_argument("--seed", type=int, default=31)
-    ap.add_argument("--tau", type=float, default=0.2)
+    ap.add_argument("--tau", type=float, default=0.1)
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--out", default=DEFAULT_MODEL)
     ap.add_argument("--model", default=None, help="evaluate: model file (default: the bundled one)")

@@ -151,17 +151,16 @@ def test_learned_policy_returns_the_same_discords_with_any_model():
 
 @pytest.mark.gpu
 def test_trained_model_saves_attempts_on_held_out_series():
-    """What the network gains: on series from a seed not used in training
-    (the held-out evaluation of the training recipe, scaled to fit the test
-    budget: 4 series of 2^18, lengths 64..320), the learned policy needs no
-    more attempts in total than the exact-bound policy alone and fewer than
-    the reference's MERLIN schedule, with identical discords."""
+    """What the network gains: on held-out series of the evaluation recipe
+    (seed 97, n = 2^20, lengths 64..1024; the model was trained on seed 31),
+    the learned r policy takes fewer attempts than the exact bound alone and
+    than the reference's MERLIN schedule, with identical discords."""
     from paddi_b200 import learned_r
-    series = datagen.training_series(4, 1 << 18, 97, min_len=64, max_len=320)
-    rows = learned_r.evaluate(series, 64, 320, model=learned_r.load_default())
-    ok = [r for r in rows if all(r[p] is not None for p in r)]
-    assert len(ok) >= 3  # MERLIN may hit its attempt cap on a series (S vanishes)
-    tot = {p: sum(r[p]["attempts"] for r in ok) for p in ("merlin", "bound", "learned")}
-    assert all(r[p]["same"] for r in ok for p in r)
-    assert tot["learned"] <= tot["bound"], tot
-    assert tot["learned"] < tot["merlin"], tot
+    series = datagen.training_series(2, 1 << 20, 97, min_len=64, max_len=1024)
+    rows = learned_r.evaluate(series, 64, 1024, model=learned_r.load_default())
+    for r in rows:
+        assert all(r[p] is not None and r[p]["same"] for p in r), r
+        assert r["learned"]["attempts"] <= r["bound"]["attempts"], r
+        assert r["learned"]["attempts"] < r["merlin"]["attempts"], r
+    tot = {p: sum(r[p]["attempts"] for r in rows) for p in ("merlin", "bound", "learned")}
+    assert tot["learned"] < tot["bound"] < tot["merlin"], tot
