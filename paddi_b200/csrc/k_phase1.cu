@@ -94,8 +94,9 @@ __device__ __forceinline__ float warp_max(float v)
 __device__ __forceinline__ float norm_up(float n) { return n * (1.f + 2.f * kU); }
 
 struct P1Smem {
-    float4 *rowdg;    // R: {df, df, dg, dg} of the row
-    float2 *rowt;     // R: {-T, -T}, T = thr * n_i
+    float4 *rowdg;    // R: {df, dg, -T, 0} of the row, T = thr * n_i (one entry: more
+                      // tasks fit an SM's shared memory; the packed pairs are built
+                      // in registers)
     float2 *colz;     // ncp: (inv_q, inv_q+H)
     float4 *colxy;    // ncp: (df_q, df_q+H, dg_q, dg_q+H)
     float2 *xa2;      // mpad: (a_q, a_q), the centred first row window (start dots)
@@ -130,8 +131,8 @@ __device__ __forceinline__ void p1_walk(const P1Smem &S, float2 (&cov)[P1_GPT], 
     // one row: v[k] for the 4 diagonal pairs, the row's ballot, the update
     auto row = [&](int s, int u, float2 (&v)[P1_GPT]) {
         const float4 rd = S.rowdg[s];
-        const float2 rt = S.rowt[s];
-        const float2 rix = make_float2(rd.x, rd.y), riy = make_float2(rd.z, rd.w);
+        const float2 rt = make_float2(rd.z, rd.z);
+        const float2 rix = make_float2(rd.x, rd.x), riy = make_float2(rd.y, rd.y);
 #pragma unroll
         for (int k = 0; k < P1_GPT; ++k) {
             const int sl = (u + k) & 3;
@@ -208,8 +209,7 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
     const int ncp = p1_ncp(R);
     P1Smem S;
     S.rowdg = reinterpret_cast<float4 *>(p1_smem);
-    S.rowt = reinterpret_cast<float2 *>(S.rowdg + R);
-    S.colxy = reinterpret_cast<float4 *>(S.rowt + R);
+    S.colxy = reinterpret_cast<float4 *>(S.rowdg + R);
     S.colz = reinterpret_cast<float2 *>(S.colxy + ncp);
     S.xa2 = reinterpret_cast<float2 *>(S.colxy); // start dots: aliases the column arrays
     S.xb2 = S.xa2 + mpad;
@@ -246,9 +246,8 @@ k_phase1(const float *__restrict__ x, const float4 *__restrict__ wst, const floa
         float nr = 0.f, fr = 0.f, gr = 0.f;
         for (int s = t; s < R; s += P1_THREADS) {
             const float4 w = wst[i0 + s]; // zero beyond N (padded tail)
-            S.rowdg[s] = make_float4(w.x, w.x, w.y, w.y);
             const float T = w.z > 0.f ? thr * w.w : (thr < 0.f ? -INFINITY : INFINITY);
-            S.rowt[s] = make_float2(-T, -T);
+            S.rowdg[s] = make_float4(w.x, w.y, -T, 0.f);
             S.rowflag[s] = 0;
             nr = fmaxf(nr, w.w);
             fr = fmaxf(fr, fabsf(w.x));
@@ -372,7 +371,7 @@ size_t paddi_phase1_smem(int R, int m)
 {
     const int mpad = (m + 7) & ~7;
     const int ncp = p1_ncp(R);
-    size_t b = (sizeof(float4) + sizeof(float2)) * (size_t)R; // rowdg, rowt
+    size_t b = sizeof(float4) * (size_t)R; // rowdg
     const size_t ubytes = std::max((size_t)24 * ncp, (size_t)8 * (mpad + p1_nbp(m)));
     b += (ubytes + 15) & ~(size_t)15;        // colxy + colz / xa2 + xb2
     b += (size_t)(R + P1_D) + (size_t)R;     // flags

@@ -62,7 +62,7 @@ constexpr int UM_THREADS = 384;  // 12 warps
 constexpr int UM_TCMAX = 16;     // candidates per tile (M = 128); 8 for M = 64
 constexpr int UM_N = 256;        // windows at stride 8
 constexpr int UM_TW = UM_N * 8;  // windows per tile (one block of the grid)
-constexpr int UM_WAVES = 2;      // work items per CTA and round when candidate tiles are few
+constexpr int UM_WAVES = 1;      // work items per CTA and round when candidate tiles are few
 constexpr int UM_KMAX128 = 368;  // largest K' with M = 128 (shared-memory bound)
 constexpr int UM_KMAX64 = 736;   // largest K' with M = 64
 constexpr int ZSCALE = 8;        // zhat scaled by 2^8 before splitting

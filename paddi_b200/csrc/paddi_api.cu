@@ -236,7 +236,11 @@ int refine_kernel_for(const paddi_ctx *ctx, int m)
 float guard_of(const paddi_ctx *ctx, int kernel)
 {
     if (ctx->opts.guard > 0.f) return ctx->opts.guard;
-    return kernel == PADDI_DIST_SPLIT_BF16 ? 1e-3f : 1e-4f;
+    // the largest per-window rounding bound the bounded kernels accept (above it
+    // a window is fragile and goes to the FP64 pass), and the band of the FP64
+    // recheck: 2e-4 balances the two on the headline series (1e-4 left 35k
+    // fragile windows per attempt, 4e-4 doubled the rechecks)
+    return kernel == PADDI_DIST_SPLIT_BF16 ? 1e-3f : 2e-4f;
 }
 
 // Statistics of length m for the series in `x` (n values); with `tiles`, also
