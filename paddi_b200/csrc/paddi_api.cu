@@ -231,8 +231,8 @@ int refine_kernel_for(const paddi_ctx *ctx, int m)
     return k == PADDI_DIST_SPLIT_BF16 ? PADDI_DIST_SPLIT_BF16 : PADDI_DIST_SPLIT_FP16;
 }
 
-// Correlation guard band of the pruning decisions.  FP32 and split-FP16
-// keep rho within ~1e-5; split-BF16 within ~2e-4 on random-walk slices.
+// Guard band, in correlation units: the largest per-window rounding bound a
+// bounded refine kernel accepts, and the half-width of the FP64 recheck band.
 float guard_of(const paddi_ctx *ctx, int kernel)
 {
     if (ctx->opts.guard > 0.f) return ctx->opts.guard;

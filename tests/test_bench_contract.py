@@ -35,3 +35,11 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+
+
+def test_config_runner_lists_the_reference_configurations():
+    out = subprocess.run([sys.executable, "-m", "paddi_b200.configs", "--help"], cwd=ROOT,
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    for name in ("fixed", "batched"):
+        assert name in out.stdout
