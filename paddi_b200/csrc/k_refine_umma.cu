@@ -438,7 +438,7 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
               const uint16_t *__restrict__ bq, const float4 *__restrict__ wdq,
               PaddiAttemptDev *att, int32_t *work, uint32_t *rho_max, uint8_t *pruned, int32_t N,
               int32_t m, int32_t jb, int32_t je, float thr, int32_t grid_ctas, long long wl,
-              int32_t withhold)
+              int32_t withhold, int32_t round, int32_t je_all)
 {
     using X = E16<BF>;
     constexpr int UM_M = MM;
@@ -452,7 +452,15 @@ k_refine_umma(const float *__restrict__ x, const float4 *__restrict__ wst,
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     const int C = *list_count;
-    if (C <= 0 || je <= jb) return; // uniform: before any TMEM or barrier use
+    // an earlier round with one candidate tile left took every remaining window
+    const int cov = att->covered_from;
+    if (C <= 0 || je <= jb || (cov > 0 && cov <= round)) return; // uniform, before any TMEM use
+    // one tile left: later rounds could not shrink it, so take the rest of the
+    // windows now and spare them their launches' fixed cost
+    if (C <= UM_TC && je_all > je) {
+        je = je_all;
+        if (blockIdx.x == 0 && threadIdx.x == 0) att->covered_from = round + 1;
+    }
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < 2; ++s) {
@@ -939,11 +947,14 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                                      const float4 *wdq, PaddiAttemptDev *att, int32_t *work,
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
                                      int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
-                                     cudaStream_t st, long long wait_cycles, int32_t withhold)
+                                     cudaStream_t st, long long wait_cycles, int32_t withhold,
+                                     int32_t round, int32_t je_all)
 {
     const int kp = kpad_of(m);
     if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
     if ((jb % UM_TW) != 0 || (je % UM_TW != 0 && je != N)) return cudaErrorInvalidValue;
+    if (je_all > 0 && (je_all < je || (je_all % UM_TW != 0 && je_all != N)))
+        return cudaErrorInvalidValue;
     const int MM = kp <= UM_KMAX128 ? 128 : 64;
     const UmLayout L = um_layout(MM, kp);
     // request at least half the SM's shared memory so one CTA owns the 512 TMEM columns
@@ -951,7 +962,7 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
     void (*kern)(const float *, const float4 *, const float *, const int32_t *, const int32_t *,
                  const int32_t *, const uint16_t *, const float4 *, PaddiAttemptDev *, int32_t *,
                  uint32_t *, uint8_t *, int32_t, int32_t, int32_t, int32_t, float, int32_t,
-                 long long, int32_t);
+                 long long, int32_t, int32_t, int32_t);
     if (MM == 128) kern = bf16 ? k_refine_umma<true, 128> : k_refine_umma<false, 128>;
     else kern = bf16 ? k_refine_umma<true, 64> : k_refine_umma<false, 64>;
     cudaError_t e = paddi_raise_smem_limit((const void *)kern, smem);
@@ -959,6 +970,7 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
     const int grid = num_sms;
     kern<<<grid, UM_THREADS, smem, st>>>(x, wst, mu, cand, list, list_count, bq, wdq, att, work,
                                          rho_max, pruned, N, m, jb, je, thr_prune, grid,
-                                         wait_cycles > 0 ? wait_cycles : 4000000000ll, withhold);
+                                         wait_cycles > 0 ? wait_cycles : 4000000000ll, withhold,
+                                         round, je_all > 0 ? je_all : je);
     return cudaGetLastError();
 }

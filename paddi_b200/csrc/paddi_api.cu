@@ -325,7 +325,8 @@ paddi_status refine_rounds(paddi_ctx *ctx, const float *x, int32_t N, int m, int
                                         ctx->d_cand, ctx->d_list[a], cnt, ctx->d_bq,
                                         ctx->d_wdq, ctx->d_att, &ctx->d_att->work_rd[rd],
                                         ctx->d_rho, ctx->d_pruned, N, m, jb, je, thr,
-                                        ctx->num_sms, st, ctx->wait_cycles, ctx->withhold));
+                                        ctx->num_sms, st, ctx->wait_cycles, ctx->withhold, rd,
+                                        col_hi));
         else
             CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
                                         cnt, ctx->d_att, &ctx->d_att->work_rd[rd], ctx->d_rho,

@@ -91,6 +91,8 @@ struct PaddiAttemptDev {
                             // the last); zero when the attempt starts, so the compactions
                             // between rounds need no reset
     int32_t p1_walked;      // phase-1 tasks that walked their rows (instrumentation)
+    int32_t covered_from;   // r + 1 when refine round r (one candidate tile left) took
+                            // every remaining window; later rounds then have nothing to do
     unsigned long long n_pairs; // pairs evaluated by the refine (instrumentation)
     unsigned long long n_live;  // of those, pairs of candidates still unpruned at the tile's start
 };
@@ -194,7 +196,8 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
                                      int32_t jb, int32_t je,
                                      float thr_prune, int32_t num_sms, cudaStream_t st,
-                                     long long wait_cycles = 0, int32_t withhold = 0);
+                                     long long wait_cycles = 0, int32_t withhold = 0,
+                                     int32_t round = 0, int32_t je_all = 0);
 
 // Per-length tile data of the tensor-core refine: for every block of
 // paddi_tile_width() windows, the split 16-bit series slice (bq, at most
