@@ -241,8 +241,11 @@ def full_length_point(ctx, st, x, disc, args):
     e1.synchronize()
     gpu_ms = e0.elapsed_time(e1)
     return {"what": f"one attempt at m={m} on all {len(y)} points, r^2={r * r:.4f}",
-            "series": "the headline generator (seed 1) with noise and reverse anomalies "
-                      "only; the reference's FP32 path finds no candidate on flat runs",
+            "series": "the headline generator (seed 1) with noise and reverse anomalies only "
+                      "(no flat runs)",
+            "reference_note": "the reference's one-pass FP32 window statistics lose the "
+                              "variances of this 2^21-point random walk (values to 1.7e3): "
+                              "its attempt prunes every window (cpu_found -1)",
             "cpu_s": cpu_s, "cores": 1, "gpu_ms": gpu_ms, "ratio": cpu_s * 1e3 / gpu_ms,
             "cpu_found": att["top_ind"], "gpu_found": got[0].ind if got else -1,
             "same_window": bool(got) and att["top_ind"] == got[0].ind,
