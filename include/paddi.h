@@ -328,7 +328,9 @@ typedef enum paddi_debug_key {
                                        (0: the default, about 2 s) */
     PADDI_DEBUG_WITHHOLD_STAGE = 3, /* 1: the next tensor-core refine launches never fill one
                                        pipeline stage, so a wait runs out (PADDI_ERR_CUDA) */
-    PADDI_DEBUG_LAST_PASSES = 4     /* read only: selection passes of the last attempt */
+    PADDI_DEBUG_LAST_PASSES = 4,    /* read only: selection passes of the last attempt */
+    PADDI_DEBUG_RECHECK_CAP = 5     /* capacity of the FP64 recheck queue (it grows on demand
+                                       when a selection overflows it) */
 } paddi_debug_key;
 paddi_status paddi_debug_set(paddi_ctx *ctx, int32_t key, int64_t value);
 paddi_status paddi_debug_get(paddi_ctx *ctx, int32_t key, int64_t *value);

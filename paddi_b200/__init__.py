@@ -160,6 +160,7 @@ _SIGS = {
 
 # test hooks (include/paddi.h, paddi_debug_key)
 DEBUG_FAIL_ALLOC, DEBUG_WAIT_CYCLES, DEBUG_WITHHOLD_STAGE, DEBUG_LAST_PASSES = 1, 2, 3, 4
+DEBUG_RECHECK_CAP = 5
 
 # Largest n - m + 1 accepted by compute_statistics_noalloc (include/paddi.h).
 NOALLOC_MAX_WINDOWS = 131072

@@ -314,6 +314,7 @@ k_finalize(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
     if (threadIdx.x == 0) {
         const int nr = s_nr;
         att->n_recheck = nr < rc_cap ? nr : rc_cap;
+        att->n_recheck_all = nr;
         // a status set earlier (3: a refine wait ran out) is kept: it explains
         // an overflow here and must reach the host unchanged
         if (nr > rc_cap) atomicCAS(&att->status, 0, 1);
@@ -516,7 +517,8 @@ k_select(const int32_t *__restrict__ cand, PaddiAttemptDev *att,
         res->n_cand += addc;
         res->n_disc += addd;
         res->n_sel = np;
-        res->n_recheck = nr;
+        // the full count, so the host can size the queue after an overflow
+        res->n_recheck = att->n_recheck_all;
         res->n_pairs = att->n_pairs;
         res->n_live = att->n_live;
         res->p1_walked = att->p1_walked;

@@ -1354,6 +1354,17 @@ PADDI_API paddi_status paddi_debug_set(paddi_ctx *ctx, int32_t key, int64_t valu
     case PADDI_DEBUG_WITHHOLD_STAGE:
         ctx->withhold = value != 0;
         return PADDI_OK;
+    case PADDI_DEBUG_RECHECK_CAP: {
+        if (value < 1 || value > (1 << 24) || !ctx->d_recheck) break;
+        CK(cudaSetDevice(ctx->device));
+        CK(cudaStreamSynchronize(ctx->st));
+        dfree(ctx->d_recheck);
+        dfree(ctx->d_nn64);
+        CK(dmalloc(ctx, &ctx->d_recheck, sizeof(int32_t) * (size_t)value));
+        CK(dmalloc(ctx, &ctx->d_nn64, sizeof(unsigned long long) * (size_t)value));
+        ctx->rc_cap = (int32_t)value;
+        return PADDI_OK;
+    }
     default:
         break;
     }
@@ -1368,6 +1379,7 @@ PADDI_API paddi_status paddi_debug_get(paddi_ctx *ctx, int32_t key, int64_t *val
     case PADDI_DEBUG_WAIT_CYCLES: *value = ctx->wait_cycles; return PADDI_OK;
     case PADDI_DEBUG_WITHHOLD_STAGE: *value = ctx->withhold; return PADDI_OK;
     case PADDI_DEBUG_LAST_PASSES: *value = ctx->last_passes; return PADDI_OK;
+    case PADDI_DEBUG_RECHECK_CAP: *value = ctx->rc_cap; return PADDI_OK;
     default: break;
     }
     return fail(ctx, PADDI_ERR_INVALID_ARG, "paddi_debug_get: unknown key");

@@ -84,7 +84,8 @@ struct PaddiAttemptDev {
     int32_t n_cand_p1;      // candidates after phase 1 (compacted list length)
     int32_t work_rd[4];     // work-item counters of the refine rounds (one per round)
     int32_t recheck_next;   // work-item counter of the FP64 recheck kernel
-    int32_t n_recheck;      // windows queued for the FP64 recheck
+    int32_t n_recheck;      // windows queued for the FP64 recheck (at most its capacity)
+    int32_t n_recheck_all;  // windows that needed it: above the capacity, the queue overflowed
     int32_t status;         // nonzero: a kernel hit an internal limit
     int32_t task_next;      // task counter of the phase-1 kernel
     int32_t list_count[5];  // candidate-list length entering each refine round (and after

@@ -72,3 +72,22 @@ def test_debug_hooks_reject_unknown_keys():
             ctx.debug_set(99, 1)
         with pytest.raises(P.PaddiError):
             ctx.debug_set(P.DEBUG_FAIL_ALLOC, -1)
+
+
+def test_recheck_queue_grows_when_a_selection_overflows_it():
+    """A selection that needs more exact values than the FP64 recheck queue
+    holds must report the full count, grow the queue and redo the selection
+    (a queue of one window overflows on the top-4 picks alone)."""
+    x = _series()
+    m = 64
+    with P.Context(device=0) as ctx:
+        ctx.reserve(len(x), m)
+        ctx.debug_set(P.DEBUG_RECHECK_CAP, 1)
+        got, log = ctx.pd3(x, m, top_k=4)
+        assert ctx.debug_get(P.DEBUG_RECHECK_CAP) > 1
+    want, wlog = O.pd3(x, m, top_k=4)
+    assert [d.ind for d in got] == [w[0] for w in want]
+    for d, w in zip(got, want):
+        assert abs(d.dist - w[1]) <= 1e-5 * abs(w[1])
+    assert [(e["n_cand"], e["n_disc"]) for e in log] == \
+        [(a["n_cand"], a["n_disc"]) for a in wlog]
