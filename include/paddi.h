@@ -82,6 +82,10 @@ typedef struct paddi_opts {
     uint32_t iter_cap;        /* attempts allowed per length; 0 = 200 */
     float guard;              /* correlation guard band of the FP32/BF16 decisions; 0 = default */
     uint32_t flags;           /* PADDI_FLAG_* */
+    uint32_t tile_rows;       /* rows M of the tensor-core refine's tiles (8 shifts of M/8
+                                 candidates): 0 = by length (128 while K' = m + 7 rounded
+                                 to 16 is at most 368, else 64), 64 = always 64; others:
+                                 PADDI_ERR_UNSUPPORTED.  Results do not depend on it. */
 } paddi_opts;
 
 /* paddi_opts.flags: compute the bound (paddi_attempt_log.lb) under every r
@@ -206,13 +210,14 @@ paddi_status paddi_palmad_batched(paddi_ctx *ctx, const float *const *series,
 
 /*
  * Autotuner: times PALMAD on short probe ranges of this series (three lengths at
- * the start, middle and end of minL..maxL) for every combination of phase-1
- * segment length {256, 384, 512} and phase-1 chunk depth {8, 12, 16}, checks
- * that all combinations return the same discords, installs the fastest in ctx
- * and copies the chosen options to *chosen.  ms (optional, 9 entries) receives
- * the probe time of each combination in the order segment-major.  No
- * reference counterpart (the reference fixes SEGMENT_N at compile time,
- * src/parameters.hpp:8-10).
+ * the start, middle and end of minL..maxL) for every combination of the refine's
+ * tile rows {by length, 64}, phase-1 segment length {256, 384, 512} and phase-1
+ * chunk depth {8, 12, 16}, checks that all combinations return the same
+ * discords, installs the fastest in ctx and copies the chosen options to
+ * *chosen.  ms (optional, 18 entries) receives the probe time of each
+ * combination, tile rows outermost, then segment, then chunks.  No reference
+ * counterpart (the reference fixes SEGMENT_N and its 32x32 refine tiles at
+ * compile time, src/parameters.hpp:8-10).
  */
 paddi_status paddi_autotune(paddi_ctx *ctx, const float *series, size_t n, uint32_t minL,
                             uint32_t maxL, paddi_opts *chosen, float *ms);

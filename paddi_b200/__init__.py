@@ -57,7 +57,8 @@ class _Opts(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32),
                 ("distance_kernel", C.c_int32), ("r_policy", C.c_int32),
                 ("segment_len", C.c_uint32), ("phase1_chunks", C.c_uint32),
-                ("iter_cap", C.c_uint32), ("guard", C.c_float), ("flags", C.c_uint32)]
+                ("iter_cap", C.c_uint32), ("guard", C.c_float), ("flags", C.c_uint32),
+                ("tile_rows", C.c_uint32)]
 
 
 FLAG_LOG_BOUND = 1
@@ -194,7 +195,7 @@ class Context:
     def __init__(self, device: int = 0, distance_kernel: int = DIST_AUTO,
                  r_policy: int = R_MERLIN, segment_len: int = 256, phase1_chunks: int = 12,
                  iter_cap: int = 200, guard: float = 0.0, flags: int = 0, model=None,
-                 model_margin: float = 1.0):
+                 model_margin: float = 1.0, tile_rows: int = 0):
         """model: parameters for R_LEARNED (default: the bundled trained model)."""
         L = lib()
         o = _Opts()
@@ -207,6 +208,7 @@ class Context:
         o.iter_cap = iter_cap
         o.guard = guard
         o.flags = flags
+        o.tile_rows = tile_rows
         h = C.c_void_p()
         s = L.paddi_ctx_create(C.byref(h), C.byref(o))
         if s != PADDI_OK:
@@ -335,16 +337,17 @@ class Context:
                 None if on_profile is not None else kept)
 
     def autotune(self, series, minL: int, maxL: int):
-        """Pick phase-1 segment length and depth on probe lengths of this series."""
+        """Pick the refine's tile rows and phase-1 segment length and depth on
+        probe lengths of this series."""
         x = np.ascontiguousarray(series, dtype=np.float32)
         o = _Opts()
-        ms = np.zeros(9, np.float32)
+        ms = np.zeros(18, np.float32)
         self._check(lib().paddi_autotune(self._h, x.ctypes.data, len(x), minL, maxL,
                                          C.byref(o), ms.ctypes.data))
         self.opts = o
-        grid = [(sg, ch) for sg in (256, 384, 512) for ch in (8, 12, 16)]
-        return {"segment_len": o.segment_len, "phase1_chunks": o.phase1_chunks,
-                "probe_ms": dict(zip(grid, ms.tolist()))}
+        grid = [(tr, sg, ch) for tr in (0, 64) for sg in (256, 384, 512) for ch in (8, 12, 16)]
+        return {"tile_rows": o.tile_rows, "segment_len": o.segment_len,
+                "phase1_chunks": o.phase1_chunks, "probe_ms": dict(zip(grid, ms.tolist()))}
 
     def palmad_batched(self, series_list, minL: int, maxL: int, streams: int = 4):
         """PALMAD over many uneven series; returns (discords per series, attempts)."""

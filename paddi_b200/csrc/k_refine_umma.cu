@@ -948,14 +948,14 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                                      uint32_t *rho_max, uint8_t *pruned, int32_t N, int32_t m,
                                      int32_t jb, int32_t je, float thr_prune, int32_t num_sms,
                                      cudaStream_t st, long long wait_cycles, int32_t withhold,
-                                     int32_t round, int32_t je_all)
+                                     int32_t round, int32_t je_all, bool rows64)
 {
     const int kp = kpad_of(m);
     if (kp > UM_KMAX64 || m < 3) return cudaErrorInvalidValue;
     if ((jb % UM_TW) != 0 || (je % UM_TW != 0 && je != N)) return cudaErrorInvalidValue;
     if (je_all > 0 && (je_all < je || (je_all % UM_TW != 0 && je_all != N)))
         return cudaErrorInvalidValue;
-    const int MM = kp <= UM_KMAX128 ? 128 : 64;
+    const int MM = (kp <= UM_KMAX128 && !rows64) ? 128 : 64;
     const UmLayout L = um_layout(MM, kp);
     // request at least half the SM's shared memory so one CTA owns the 512 TMEM columns
     const size_t smem = L.bytes < 120 * 1024 ? 120 * 1024 : L.bytes;

@@ -326,7 +326,7 @@ paddi_status refine_rounds(paddi_ctx *ctx, const float *x, int32_t N, int m, int
                                         ctx->d_wdq, ctx->d_att, &ctx->d_att->work_rd[rd],
                                         ctx->d_rho, ctx->d_pruned, N, m, jb, je, thr,
                                         ctx->num_sms, st, ctx->wait_cycles, ctx->withhold, rd,
-                                        col_hi));
+                                        col_hi, ctx->opts.tile_rows == 64));
         else
             CK(paddi_launch_refine_fp32(x, ctx->d_wst, ctx->d_mu, ctx->d_cand, ctx->d_list[a],
                                         cnt, ctx->d_att, &ctx->d_att->work_rd[rd], ctx->d_rho,
@@ -926,7 +926,8 @@ PADDI_API paddi_status paddi_ctx_create(paddi_ctx **out, const paddi_opts *opts)
             return PADDI_ERR_INVALID_ARG;
         }
         ctx->opts = *opts;
-        if (!segment_len_ok(ctx->opts.segment_len)) {
+        if (!segment_len_ok(ctx->opts.segment_len) ||
+            (ctx->opts.tile_rows != 0 && ctx->opts.tile_rows != 64)) {
             delete ctx;
             return PADDI_ERR_UNSUPPORTED;
         }
@@ -1625,16 +1626,18 @@ PADDI_API paddi_status paddi_autotune(paddi_ctx *ctx, const float *series, size_
         const uint32_t b = std::min(maxL, a + 2);
         if (probes.empty() || probes.back().first != a) probes.push_back({a, b});
     }
-    const uint32_t segs[3] = {256, 384, 512}, chunks[3] = {8, 12, 16};
+    const uint32_t tiles[2] = {0, 64}, segs[3] = {256, 384, 512}, chunks[3] = {8, 12, 16};
     const paddi_opts saved = ctx->opts;
     std::vector<std::vector<paddi_discord>> ref;
     float best = FLT_MAX;
     paddi_opts best_opts = saved;
     std::vector<paddi_discord> out(3);
     int idx = 0;
-    for (uint32_t sg : segs)
+    for (uint32_t tr : tiles)
+        for (uint32_t sg : segs)
         for (uint32_t ch : chunks) {
             ctx->opts = saved;
+            ctx->opts.tile_rows = tr;
             ctx->opts.segment_len = sg;
             ctx->opts.phase1_chunks = ch;
             // one untimed pass (kernel attributes, caches), then the timed one

@@ -198,7 +198,8 @@ cudaError_t paddi_launch_refine_umma(bool bf16, const float *x, const float4 *ws
                                      int32_t jb, int32_t je,
                                      float thr_prune, int32_t num_sms, cudaStream_t st,
                                      long long wait_cycles = 0, int32_t withhold = 0,
-                                     int32_t round = 0, int32_t je_all = 0);
+                                     int32_t round = 0, int32_t je_all = 0,
+                                     bool rows64 = false);
 
 // Per-length tile data of the tensor-core refine: for every block of
 // paddi_tile_width() windows, the split 16-bit series slice (bq, at most

@@ -60,6 +60,16 @@ def test_null_arguments_are_rejected_without_a_device():
                                                           P.PADDI_ERR_NO_DEVICE)
 
 
+def test_unsupported_tile_rows_are_refused_without_a_device():
+    L = P.lib()
+    o = P._Opts()
+    L.paddi_opts_default(C.byref(o))
+    assert o.tile_rows == 0
+    o.tile_rows = 128  # only 0 (by length) and 64 are accepted
+    h = C.c_void_p()
+    assert L.paddi_ctx_create(C.byref(h), C.byref(o)) == P.PADDI_ERR_UNSUPPORTED
+
+
 def test_cli_usage_without_arguments():
     import subprocess
     exe = os.path.join(ROOT, "paddi_b200", "paddi-main")

@@ -279,6 +279,25 @@ def test_refine_kernels_match_oracle(dist, n, m):
                 assert _close(d.dist, s[1])
 
 
+@pytest.mark.parametrize("dist", ["fp16", "bf16"])
+@pytest.mark.parametrize("n,m", [(8192, 64), (20000, 200), (12000, 361)])
+def test_refine_with_64_row_tiles_matches_oracle(dist, n, m):
+    """The refine's tile rows forced to 64 (8 candidates per tile) where the
+    length would pick 128: same counts and discords."""
+    dk = {"fp16": P.DIST_SPLIT_FP16, "bf16": P.DIST_SPLIT_BF16}[dist]
+    x = _series(n, 100 + m)
+    nn, _ = O.nn_profile(x, m)
+    with P.Context(distance_kernel=dk, tile_rows=64) as c:
+        r2 = float(np.float32(np.quantile(nn, 0.995)))
+        r = float(np.sqrt(np.float32(r2)))
+        att, sel = O.select(nn, m, float(np.float32(r) * np.float32(r)), top_k=2)
+        got, log = c.pd3(x, m, top_k=2, r=r)
+        assert (log[0]["n_cand"], log[0]["n_disc"]) == (att["n_cand"], att["n_disc"])
+        assert [d.ind for d in got] == [s[0] for s in sel]
+        for d, s in zip(got, sel):
+            assert _close(d.dist, s[1])
+
+
 # -------------------------------------------- r policies change work, not results
 @pytest.mark.parametrize("policy", ["bound"])
 def test_r_policy_gives_the_same_discords(policy):
@@ -396,6 +415,8 @@ def test_autotune_picks_a_config_and_keeps_results():
     with P.Context() as c:
         cfg = c.autotune(x, 48, 60)
         assert cfg["segment_len"] in (256, 384, 512) and cfg["phase1_chunks"] in (8, 12, 16)
+        assert cfg["tile_rows"] in (0, 64)
+        assert len(cfg["probe_ms"]) == 18
         assert all(v > 0 for v in cfg["probe_ms"].values())
         got, _ = c.palmad(x, 48, 60)
     want, _ = O.palmad(x, 48, 60)
