@@ -80,7 +80,11 @@ typedef struct paddi_opts {
                                  else 64..4096 (others: PADDI_ERR_UNSUPPORTED) */
     uint32_t phase1_chunks;   /* 256-diagonal chunks a segment scans before the refine; 0 = 12 */
     uint32_t iter_cap;        /* attempts allowed per length; 0 = 200 */
-    float guard;              /* correlation guard band of the FP32/BF16 decisions; 0 = default */
+    float guard;              /* guard band in correlation units: the largest per-window
+                                 rounding bound the FP32 / split-16-bit refines accept (a
+                                 window above it is evaluated in FP64) and the half-width
+                                 of the FP64 recheck band; 0 = default (2e-4; 1e-3 for
+                                 split-BF16) */
     uint32_t flags;           /* PADDI_FLAG_* */
     uint32_t tile_rows;       /* rows M of the tensor-core refine's tiles (8 shifts of M/8
                                  candidates): 0 = by length (128 while K' = m + 7 rounded
