@@ -90,3 +90,19 @@ def test_segment_lengths_beyond_the_supported_range_are_refused():
     with pytest.raises(P.PaddiError) as e:
         P.Context(device=0, segment_len=32)
     assert e.value.status == P.PADDI_ERR_UNSUPPORTED
+
+
+def test_large_run_reports_exact_distances_at_sampled_lengths():
+    """Config C5 at full size (ECG-like n = 2^27, lengths 128..384, learned r):
+    every length finds its discord, and at 8 lengths spread over the range the
+    reported distance is the FP64 nn of the reported window (a full FP64
+    profile is out of reach at this size: one length is ~1e16 pair terms)."""
+    x, _ = datagen.ecg_series(n=1 << 27, seed=5)
+    minL, maxL = 128, 384
+    with P.Context(device=0, r_policy=P.R_LEARNED) as ctx:
+        disc, log = ctx.palmad(x, minL, maxL)
+    assert {e["m"] for e in log if e["found"]} == set(range(minL, maxL + 1))
+    for m in (128, 129, 160, 200, 256, 300, 350, 384):
+        d = disc[m - minL]
+        nn, _ = O.windows_nn(x, m, [d.ind])
+        assert _close(d.dist, float(np.float32(nn[0]))), (m, d, nn[0])
