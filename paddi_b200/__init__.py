@@ -15,6 +15,7 @@ reference (PADDi src/)                                 paddi_b200
 ``do_PD3`` flags / nnDist on device, PD3.cuh:15         :meth:`Context.do_pd3`
 ``compute_statistics``, preprocessing.cuh:68            :meth:`Context.compute_statistics`
 ``struct Discord``, PALMAD_types.hpp:7                  :class:`Discord`
+fragments + all-to-all + MIN, MPI_transfers.hpp:29-84   :mod:`paddi_b200.sharded`
 =====================================================  ============================
 """
 from __future__ import annotations
