@@ -19,8 +19,16 @@
 namespace {
 
 constexpr int ST_THREADS = 256;
-constexpr int ST_TILE = 512;  // windows per CTA
+constexpr int ST_TILE = 2048; // windows per CTA (the staged halo of m values is amortised over them)
 constexpr int ST_MAXM = 1024; // longest supported window
+
+// dynamic shared memory of one CTA for length m: P1, P2 (FP64 prefixes), E
+// (int prefix of equal neighbours) and the staged values, ST_TILE + m + 2 each
+__host__ __device__ inline size_t st_smem(int m)
+{
+    const size_t L = (size_t)ST_TILE + (size_t)m + 2;
+    return L * (2 * sizeof(double) + sizeof(int) + sizeof(float));
+}
 
 // Exclusive-to-inclusive block scan over `cnt` per-thread partials.
 template <typename T>
@@ -57,10 +65,12 @@ k_window_stats(const float *__restrict__ x, int64_t n, int32_t m, int32_t N, flo
                int32_t *flat_span)
 {
     // staged values: x[t0 .. t0 + ST_TILE + m] (one extra window for mu_{i+1})
-    __shared__ double P1[ST_TILE + ST_MAXM + 2];
-    __shared__ double P2[ST_TILE + ST_MAXM + 2];
-    __shared__ int E[ST_TILE + ST_MAXM + 2];
-    __shared__ float xs[ST_TILE + ST_MAXM + 2];
+    extern __shared__ __align__(16) unsigned char st_mem[];
+    const int LS = ST_TILE + m + 2;
+    double *P1 = reinterpret_cast<double *>(st_mem);
+    double *P2 = P1 + LS;
+    int *E = reinterpret_cast<int *>(P2 + LS);
+    float *xs = reinterpret_cast<float *>(E + LS);
     __shared__ double wtot_d[ST_THREADS / 32];
     __shared__ int wtot_i[ST_THREADS / 32];
 
@@ -178,7 +188,10 @@ cudaError_t paddi_launch_stats(const float *x, int64_t n, int32_t m, float4 *wst
     const int32_t N = (int32_t)(n - m + 1);
     const int64_t total = (int64_t)N + PADDI_PAD_WIN;
     const unsigned grid = (unsigned)((total + ST_TILE - 1) / ST_TILE);
-    k_window_stats<<<grid, ST_THREADS, 0, st>>>(x, n, m, N, wst, mu, mu64, inv64, flat,
-                                                flat_count, flat_span);
+    const size_t smem = st_smem(m);
+    cudaError_t e = paddi_raise_smem_limit((const void *)k_window_stats, smem);
+    if (e != cudaSuccess) return e;
+    k_window_stats<<<grid, ST_THREADS, smem, st>>>(x, n, m, N, wst, mu, mu64, inv64, flat,
+                                                   flat_count, flat_span);
     return cudaGetLastError();
 }
