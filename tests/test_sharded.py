@@ -94,3 +94,31 @@ def test_two_gloo_ranks_give_the_single_process_pd3_topk():
     for _, disc, counts in res:
         assert [d[0] for d in disc] == [w[0] for w in want]
         assert counts == [(a["n_cand"], a["n_disc"]) for a in watt]
+
+
+def test_three_thread_ranks_give_the_single_process_palmad():
+    """The same driver with ranks as threads of one process (ThreadComm): three
+    uneven shards, the exact CPU backend per rank."""
+    import threading
+
+    from oracle import oracle as O
+    from tests.shard_oracle import OracleBackend
+    x = _series()
+    comms = sharded.ThreadComm.group(3)
+    res = [None] * 3
+
+    def run(rank):
+        disc, logs = sharded.palmad_sharded(OracleBackend(x, seed=rank), comms[rank], 40, 45)
+        res[rank] = ([(d.ind, d.dist) for d in disc], [(e["n_cand"], e["n_disc"]) for e in logs])
+
+    ts = [threading.Thread(target=run, args=(r,)) for r in range(3)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(300)
+    want, watt = O.palmad(x, 40, 45)
+    for disc, counts in res:
+        assert [d[0] for d in disc] == [w[0] for w in want]
+        for d, w in zip(disc, want):
+            assert abs(d[1] - w[1]) <= 1e-6 * abs(w[1])
+        assert counts == [(a["n_cand"], a["n_disc"]) for a in watt]
